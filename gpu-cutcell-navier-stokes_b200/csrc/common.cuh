@@ -1,0 +1,106 @@
+// Shared device utilities: status codes, bounded grid barrier, deterministic
+// block / grid reductions, storage-type conversions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "../../include/cutcell_b200.h"
+
+#ifndef CUTCELL_BLOCK
+#define CUTCELL_BLOCK 256
+#endif
+#define CUTCELL_WARPS (CUTCELL_BLOCK / 32)
+
+// Grid barrier wait limit in SM clock cycles (about one second at 2 GHz).  A
+// barrier that runs out sets CUTCELL_E_BARRIER and every block leaves its loop.
+#define CUTCELL_BARRIER_CYCLES 2000000000LL
+
+struct GridSync {
+    unsigned* count;
+    unsigned* gen;
+    int* err;
+    unsigned nblocks;
+};
+
+__device__ __forceinline__ int grid_error(const GridSync& gs) {
+    return *((volatile int*)gs.err);
+}
+
+// Sense-free generation barrier for a cooperative (co-resident) grid.  Every
+// wait is bounded; on timeout the error word is set and the caller returns.
+__device__ __forceinline__ bool grid_sync(const GridSync& gs) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = gs.gen;
+        unsigned g = *vgen;
+        __threadfence();
+        unsigned arrived = atomicAdd(gs.count, 1u);
+        if (arrived == gs.nblocks - 1) {
+            atomicExch(gs.count, 0u);
+            __threadfence();
+            atomicAdd(gs.gen, 1u);
+        } else {
+            long long t0 = clock64();
+            while (*vgen == g) {
+                if (clock64() - t0 > CUTCELL_BARRIER_CYCLES) {
+                    atomicExch(gs.err, CUTCELL_E_BARRIER);
+                    break;
+                }
+                if (*((volatile int*)gs.err) != 0) break;
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return grid_error(gs) == 0;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum (fixed tree); result broadcast to all threads.
+// ``sh`` needs CUTCELL_WARPS doubles.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double t = (threadIdx.x < CUTCELL_WARPS) ? sh[threadIdx.x] : 0.0;
+    if (w == 0) t = warp_sum(t);
+    if (threadIdx.x == 0) sh[0] = t;
+    __syncthreads();
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// Sum of nblocks partials written at part[0..nblocks-1], in a fixed order so
+// every block obtains the bit-identical value.
+__device__ __forceinline__ double grid_reduce(const double* part, int nblocks, double* sh) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += blockDim.x) s += ((volatile const double*)part)[i];
+    return block_sum(s, sh);
+}
+
+template <typename T> struct Conv;
+template <> struct Conv<double> {
+    typedef double acc;
+    __device__ __forceinline__ static double ld(const double* p) { return __ldg(p); }
+};
+template <> struct Conv<float> {
+    typedef float acc;
+    __device__ __forceinline__ static float ld(const float* p) { return __ldg(p); }
+};
+template <> struct Conv<__nv_bfloat16> {
+    typedef float acc;
+    __device__ __forceinline__ static float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+};
+
+static inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }

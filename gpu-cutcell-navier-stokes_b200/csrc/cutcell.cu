@@ -1,0 +1,450 @@
+// C ABI of libcutcell_b200.so: contexts, cooperative launches, status codes.
+// The persistent kernels live in pcg.cuh / ops.cuh.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "pcg.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return CUTCELL_E_CUDA;
+}
+
+#define CK(call)                                          \
+    do {                                                  \
+        cudaError_t _e = (call);                          \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+    } while (0)
+
+enum { KIND_CSR = 0, KIND_TILES = 1 };
+
+__global__ void csr_diag_inv_kernel(int n, const int* ptr, const int* idx, const double* val, double* dinv) {
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int k = ptr[row]; k < ptr[row + 1]; ++k)
+            if (idx[k] == row) d += val[k];
+        dinv[row] = (fabs(d) > 0.0) ? 1.0 / d : 1.0;
+    }
+}
+
+__global__ void fill_kernel(int n, double v, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = v;
+}
+
+__global__ void diag_inv_kernel(int n, const double* diag, double* dinv) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double d = diag[i];
+        dinv[i] = (fabs(d) > 0.0) ? 1.0 / d : 1.0;
+    }
+}
+
+__global__ void to_f32_kernel(size_t n, const double* in, float* out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+__global__ void to_bf16_kernel(size_t n, const double* in, __nv_bfloat16* out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = __float2bfloat16((float)in[i]);
+}
+
+__global__ void ext_gather_kernel(ExtDev e, const double* xr, double* xf) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < e.n_full; i += gridDim.x * blockDim.x)
+        xf[i] = e.gather(xr, i);
+}
+
+__global__ void ext_scatter_kernel(ExtDev e, const double* yf, double* yr) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < e.n_red; j += gridDim.x * blockDim.x) {
+        double y = yf[e.full_of_red[j]];
+        for (int k = e.smallT_ptr[j]; k < e.smallT_ptr[j + 1]; ++k) y += e.smallT_val[k] * yf[e.smallT_row[k]];
+        yr[j] = y;
+    }
+}
+
+template <class K>
+int occupancy_blocks(K kernel, size_t smem, int* out) {
+    int dev = 0, sms = 0, per = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, CUTCELL_BLOCK, smem));
+    if (per < 1) {
+        g_last_error = "kernel does not fit on an SM";
+        return CUTCELL_E_CUDA;
+    }
+    *out = sms * per;
+    return CUTCELL_OK;
+}
+
+}  // namespace
+
+struct cutcell_ctx {
+    int kind = KIND_CSR;
+    int n = 0;
+    int device = 0;
+    // CSR
+    CsrOp<double> csr64;
+    CsrOp<float> csr32;
+    CsrOp<__nv_bfloat16> csr16;
+    float* val32 = nullptr;
+    __nv_bfloat16* val16 = nullptr;
+    // tiles
+    TileOp<double> t64;
+    TileOp<float> t32;
+    TileOp<__nv_bfloat16> t16;
+    float* cut32 = nullptr;
+    __nv_bfloat16* cut16 = nullptr;
+    double* ypart = nullptr;
+    size_t tile_smem = 0;
+    // scratch
+    double* dinv = nullptr;
+    double* ones = nullptr;
+    bool use_jacobi = true;
+    double* r = nullptr;
+    double* p = nullptr;
+    double* Ap = nullptr;
+    double* d = nullptr;
+    double* rhat = nullptr;
+    double* part = nullptr;
+    unsigned* bar = nullptr;  // [0] count, [1] gen, [2] err (int)
+    DevResult* res = nullptr;
+    int max_blocks = 0;
+    // refinement
+    double inner_tol = 1e-4;
+    int inner_maxiter = 100000;
+    int max_outer = 50;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static int alloc_scratch(cutcell_ctx* c) {
+    const size_t nb = (size_t)c->n * sizeof(double);
+    CK(cudaMalloc(&c->dinv, nb));
+    CK(cudaMalloc(&c->ones, nb));
+    fill_kernel<<<ceil_div(c->n, 256), 256>>>(c->n, 1.0, c->ones);
+    CK(cudaMalloc(&c->r, nb));
+    CK(cudaMalloc(&c->p, nb));
+    CK(cudaMalloc(&c->Ap, nb));
+    CK(cudaMalloc(&c->d, nb));
+    CK(cudaMalloc(&c->rhat, nb));
+    CK(cudaMalloc(&c->bar, 4 * sizeof(unsigned)));
+    CK(cudaMalloc(&c->res, sizeof(DevResult)));
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+    return CUTCELL_OK;
+}
+
+template <class K>
+static int ensure_part(cutcell_ctx* c, K kernel, size_t smem, int* blocks) {
+    int st = occupancy_blocks(kernel, smem, blocks);
+    if (st) return st;
+    if (*blocks > c->max_blocks) {
+        if (c->part) cudaFree(c->part);
+        c->part = nullptr;
+        CK(cudaMalloc(&c->part, (size_t)8 * (*blocks) * sizeof(double)));
+        c->max_blocks = *blocks;
+    }
+    return CUTCELL_OK;
+}
+
+static GridSync make_gs(cutcell_ctx* c, int blocks) {
+    GridSync gs;
+    gs.count = c->bar;
+    gs.gen = c->bar + 1;
+    gs.err = (int*)(c->bar + 2);
+    gs.nblocks = (unsigned)blocks;
+    return gs;
+}
+
+static PcgBufs make_bufs(cutcell_ctx* c) {
+    PcgBufs B;
+    B.n = c->n;
+    B.dinv = c->use_jacobi ? c->dinv : c->ones;
+    B.r = c->r;
+    B.p = c->p;
+    B.Ap = c->Ap;
+    B.part = c->part;
+    return B;
+}
+
+template <class K, class... Args>
+static int launch_coop(K kernel, int blocks, size_t smem, cudaStream_t s, Args... args) {
+    void* ptrs[] = {(void*)&args...};
+    CK(cudaLaunchCooperativeKernel((const void*)kernel, dim3(blocks), dim3(CUTCELL_BLOCK), ptrs, smem, s));
+    return CUTCELL_OK;
+}
+
+template <class Op>
+static int run_plain(cutcell_ctx* c, const Op& op, size_t smem, SolveArgs& a, cudaStream_t s, int* blocks) {
+    auto kern = pcg_kernel<Op>;
+    int st = ensure_part(c, kern, smem, blocks);
+    if (st) return st;
+    a.gs = make_gs(c, *blocks);
+    a.B = make_bufs(c);
+    return launch_coop(kern, *blocks, smem, s, op, a);
+}
+
+template <class OpHi, class OpLo>
+static int run_ir(cutcell_ctx* c, const OpHi& hi, const OpLo& lo, size_t smem, SolveArgs& a, cudaStream_t s,
+                  int* blocks) {
+    auto kern = ir_kernel<OpHi, OpLo>;
+    int st = ensure_part(c, kern, smem, blocks);
+    if (st) return st;
+    a.gs = make_gs(c, *blocks);
+    a.B = make_bufs(c);
+    return launch_coop(kern, *blocks, smem, s, hi, lo, a);
+}
+
+template <class Op>
+static int run_apply(cutcell_ctx* c, const Op& op, size_t smem, const double* x, double* y, cudaStream_t s) {
+    auto kern = apply_kernel<Op>;
+    int blocks = 0;
+    int st = ensure_part(c, kern, smem, &blocks);
+    if (st) return st;
+    CK(cudaMemsetAsync(c->bar, 0, 4 * sizeof(unsigned), s));
+    GridSync gs = make_gs(c, blocks);
+    return launch_coop(kern, blocks, smem, s, op, x, y, gs);
+}
+
+extern "C" {
+
+const char* cutcell_status_string(int status) {
+    switch (status) {
+        case CUTCELL_OK: return "converged";
+        case CUTCELL_E_NOCONV: return "maximum iterations reached";
+        case CUTCELL_E_BREAKDOWN: return "CG breakdown: non-positive curvature";
+        case CUTCELL_E_NAN: return "non-finite residual";
+        case CUTCELL_E_SHAPE: return "inconsistent sizes";
+        case CUTCELL_E_CUDA: return "CUDA runtime error";
+        case CUTCELL_E_BARRIER: return "device-wide wait timed out";
+        case CUTCELL_E_ARG: return "invalid argument";
+        default: return "unknown status";
+    }
+}
+
+const char* cutcell_last_error(void) { return g_last_error.c_str(); }
+
+int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const int32_t* indices, const double* data,
+                           cutcell_ctx** out) {
+    if (!out || n <= 0 || nnz < 0 || !indptr || (nnz > 0 && (!indices || !data))) return CUTCELL_E_ARG;
+    cutcell_ctx* c = new cutcell_ctx();
+    c->kind = KIND_CSR;
+    c->n = n;
+    CK(cudaGetDevice(&c->device));
+    int st = alloc_scratch(c);
+    if (st) {
+        delete c;
+        return st;
+    }
+    // threads per row from the mean row length (power of two in [1, 32])
+    const double mean = nnz / (double)n;
+    int l2 = 0;
+    while ((1 << l2) < 32 && (1 << l2) * 2 <= mean) ++l2;
+    c->csr64 = CsrOp<double>{n, l2, indptr, indices, data};
+    if (nnz > 0) {
+        CK(cudaMalloc(&c->val32, (size_t)nnz * sizeof(float)));
+        CK(cudaMalloc(&c->val16, (size_t)nnz * sizeof(__nv_bfloat16)));
+        to_f32_kernel<<<592, 256>>>((size_t)nnz, data, c->val32);
+        to_bf16_kernel<<<592, 256>>>((size_t)nnz, data, c->val16);
+    }
+    c->csr32 = CsrOp<float>{n, l2, indptr, indices, c->val32};
+    c->csr16 = CsrOp<__nv_bfloat16>{n, l2, indptr, indices, c->val16};
+    csr_diag_inv_kernel<<<ceil_div(n, 256), 256>>>(n, indptr, indices, data, c->dinv);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    *out = c;
+    return CUTCELL_OK;
+}
+
+int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
+    if (!out || !t) return CUTCELL_E_ARG;
+    const int p = t->degree, P1 = p + 1, P = P1 * P1 * P1, D = t->tile + p;
+    const int nb = t->n_elements + p;
+    if (p < 1 || t->tile < 1 || t->n_tiles_axis * t->tile < t->n_elements || (long)nb * nb * nb != t->n_full ||
+        t->n_red <= 0)
+        return CUTCELL_E_SHAPE;
+    cutcell_ctx* c = new cutcell_ctx();
+    c->kind = KIND_TILES;
+    c->n = t->n_red;
+    CK(cudaGetDevice(&c->device));
+    int st = alloc_scratch(c);
+    if (st) {
+        delete c;
+        return st;
+    }
+    const size_t nt3 = (size_t)t->n_tiles_axis * t->n_tiles_axis * t->n_tiles_axis;
+    CK(cudaMalloc(&c->ypart, nt3 * D * D * D * sizeof(double)));
+    CK(cudaMemset(c->ypart, 0, nt3 * D * D * D * sizeof(double)));
+    const size_t ncm = (size_t)t->n_cut * P * P;
+    if (ncm) {
+        CK(cudaMalloc(&c->cut32, ncm * sizeof(float)));
+        CK(cudaMalloc(&c->cut16, ncm * sizeof(__nv_bfloat16)));
+        to_f32_kernel<<<592, 256>>>(ncm, t->cut_mats, c->cut32);
+        to_bf16_kernel<<<592, 256>>>(ncm, t->cut_mats, c->cut16);
+    }
+    ExtDev e;
+    e.n_full = t->n_full;
+    e.n_red = t->n_red;
+    e.n_small = t->n_small;
+    e.red_of_full = t->red_of_full;
+    e.small_slot = t->small_slot;
+    e.small_ptr = t->small_ptr;
+    e.small_idx = t->small_idx;
+    e.small_val = t->small_val;
+    e.full_of_red = t->full_of_red;
+    e.smallT_ptr = t->smallT_ptr;
+    e.smallT_row = t->smallT_row;
+    e.smallT_val = t->smallT_val;
+    TileOp<double> o;
+    o.n = t->n_elements;
+    o.p = p;
+    o.P1 = P1;
+    o.P = P;
+    o.T = t->tile;
+    o.D = D;
+    o.nta = t->n_tiles_axis;
+    o.nb = nb;
+    o.ntile_list = t->n_tile_list;
+    o.a_mass = t->a_mass;
+    o.tile_list = t->tile_list;
+    o.tile_kind = t->tile_kind;
+    o.tile_eptr = t->tile_eptr;
+    o.tile_elem = t->tile_elem;
+    o.tile_ecut = t->tile_ecut;
+    o.M1 = t->M1;
+    o.Kt1 = t->Kt1;
+    o.TM = t->TM;
+    o.TA = t->TA;
+    o.TK = t->TK;
+    o.cut_mats = t->cut_mats;
+    o.ext = e;
+    o.ypart = c->ypart;
+    c->t64 = o;
+    // same geometry, reduced-precision cut blocks
+    memcpy(&c->t32, &o, sizeof(o));
+    c->t32.cut_mats = c->cut32;
+    memcpy(&c->t16, &o, sizeof(o));
+    c->t16.cut_mats = c->cut16;
+    c->tile_smem = TileOp<double>::smem_bytes(D, P, CUTCELL_WARPS);
+    diag_inv_kernel<<<ceil_div(t->n_red, 256), 256>>>(t->n_red, t->diag, c->dinv);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    *out = c;
+    return CUTCELL_OK;
+}
+
+int cutcell_set_refinement(cutcell_ctx* c, double inner_tol, int32_t inner_maxiter, int32_t max_outer) {
+    if (!c || !(inner_tol > 0.0) || inner_maxiter < 1 || max_outer < 1) return CUTCELL_E_ARG;
+    c->inner_tol = inner_tol;
+    c->inner_maxiter = inner_maxiter;
+    c->max_outer = max_outer;
+    return CUTCELL_OK;
+}
+
+int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, int32_t maxiter, int32_t precision,
+                      int32_t precond, CutcellReport* report, void* stream) {
+    if (!c || !b || !x || maxiter < 0 || !(tol >= 0.0)) return CUTCELL_E_ARG;
+    if (precision < CUTCELL_FP64 || precision > CUTCELL_BF16_IR) return CUTCELL_E_ARG;
+    if (precond != CUTCELL_PRECOND_NONE && precond != CUTCELL_PRECOND_JACOBI) return CUTCELL_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaSetDevice(c->device));
+    c->use_jacobi = (precond == CUTCELL_PRECOND_JACOBI);
+    SolveArgs a;
+    memset(&a, 0, sizeof(a));
+    a.b = b;
+    a.x = x;
+    a.tol = tol;
+    a.maxiter = maxiter;
+    a.inner_tol = c->inner_tol;
+    a.inner_maxiter = c->inner_maxiter;
+    a.max_outer = c->max_outer;
+    a.d = c->d;
+    a.rhat = c->rhat;
+    a.res = c->res;
+    CK(cudaMemsetAsync(c->bar, 0, 4 * sizeof(unsigned), s));
+    CK(cudaEventRecord(c->ev0, s));
+    int blocks = 0;
+    int st = CUTCELL_OK;
+    if (c->kind == KIND_CSR) {
+        if (precision == CUTCELL_FP64)
+            st = run_plain(c, c->csr64, 0, a, s, &blocks);
+        else if (precision == CUTCELL_FP32_IR)
+            st = run_ir(c, c->csr64, c->csr32, 0, a, s, &blocks);
+        else
+            st = run_ir(c, c->csr64, c->csr16, 0, a, s, &blocks);
+    } else {
+        const size_t sm = c->tile_smem;
+        if (precision == CUTCELL_FP64)
+            st = run_plain(c, c->t64, sm, a, s, &blocks);
+        else if (precision == CUTCELL_FP32_IR)
+            st = run_ir(c, c->t64, c->t32, sm, a, s, &blocks);
+        else
+            st = run_ir(c, c->t64, c->t16, sm, a, s, &blocks);
+    }
+    if (st) return st;
+    CK(cudaEventRecord(c->ev1, s));
+    DevResult hr;
+    CK(cudaMemcpyAsync(&hr, c->res, sizeof(hr), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (report) {
+        report->status = hr.status;
+        report->iterations = hr.iterations;
+        report->outer_iterations = hr.outer;
+        report->blocks = blocks;
+        report->relative_residual = hr.rel;
+        report->true_relative_residual = hr.true_rel;
+        report->elapsed_ms = ms;
+    }
+    return hr.status == CUTCELL_E_BARRIER ? CUTCELL_E_BARRIER : CUTCELL_OK;
+}
+
+int cutcell_apply(cutcell_ctx* c, const double* x, double* y, int32_t precision, void* stream) {
+    if (!c || !x || !y) return CUTCELL_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (c->kind == KIND_CSR) {
+        if (precision == CUTCELL_FP64) return run_apply(c, c->csr64, 0, x, y, s);
+        if (precision == CUTCELL_FP32_IR) return run_apply(c, c->csr32, 0, x, y, s);
+        if (precision == CUTCELL_BF16_IR) return run_apply(c, c->csr16, 0, x, y, s);
+    } else {
+        if (precision == CUTCELL_FP64) return run_apply(c, c->t64, c->tile_smem, x, y, s);
+        if (precision == CUTCELL_FP32_IR) return run_apply(c, c->t32, c->tile_smem, x, y, s);
+        if (precision == CUTCELL_BF16_IR) return run_apply(c, c->t16, c->tile_smem, x, y, s);
+    }
+    return CUTCELL_E_ARG;
+}
+
+int cutcell_ext_gather(cutcell_ctx* c, const double* x_red, double* x_full, void* stream) {
+    if (!c || c->kind != KIND_TILES || !x_red || !x_full) return CUTCELL_E_ARG;
+    ext_gather_kernel<<<ceil_div(c->t64.ext.n_full, 256), 256, 0, (cudaStream_t)stream>>>(c->t64.ext, x_red, x_full);
+    CK(cudaGetLastError());
+    return CUTCELL_OK;
+}
+
+int cutcell_ext_scatter(cutcell_ctx* c, const double* y_full, double* y_red, void* stream) {
+    if (!c || c->kind != KIND_TILES || !y_full || !y_red) return CUTCELL_E_ARG;
+    ext_scatter_kernel<<<ceil_div(c->t64.ext.n_red, 256), 256, 0, (cudaStream_t)stream>>>(c->t64.ext, y_full, y_red);
+    CK(cudaGetLastError());
+    return CUTCELL_OK;
+}
+
+int cutcell_destroy(cutcell_ctx* c) {
+    if (!c) return CUTCELL_E_ARG;
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->dinv, c->ones, c->r,
+                    c->p,     c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    delete c;
+    return CUTCELL_OK;
+}
+
+}  // extern "C"

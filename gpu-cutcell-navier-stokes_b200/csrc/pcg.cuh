@@ -1,0 +1,258 @@
+// Persistent Jacobi-PCG and FP64 iterative refinement, one cooperative launch
+// per solve.  The iteration is the one of solve_gpu_cg
+// (code/fast_solver_backends.py:236-274):
+//
+//   x = 0, r = b, z = D^{-1} r (z = r where the diagonal is zero), p = z
+//   loop k = 1..maxiter:
+//     Ap = A p; pAp = p.Ap; stop "breakdown" if pAp <= 0 or non-finite
+//     alpha = rz/pAp; x += alpha p; r -= alpha Ap
+//     stop "converged" if ||r||/||b|| <= tol (iterations = k)
+//     z = D^{-1} r; beta = rz_new/rz; p = z + beta p
+//
+// Every dot product is a deterministic two-level reduction (block tree, then
+// a fixed-order sum of the per-block partials that every block repeats), so
+// all blocks take identical branch decisions and reruns are bit-identical.
+#pragma once
+
+#include "ops.cuh"
+
+struct DevResult {
+    int status;
+    int iterations;
+    int outer;
+    int pad;
+    double rel;
+    double true_rel;
+};
+
+struct PcgBufs {
+    int n;
+    const double* dinv;  // Jacobi inverse (1 where the diagonal is zero)
+    double* r;
+    double* p;
+    double* Ap;
+    double* part;        // [8][nblocks]
+};
+
+// Inner PCG on A d = rhs from d = 0.  Returns the status; *iters receives the
+// iteration count and *rel the final recursive relative residual.
+template <class Op>
+__device__ int pcg_core(const Op& op, const PcgBufs& B, const double* rhs, double* d, double tol, int maxiter,
+                        const GridSync& gs, double* sm, double* sh, double rhs_norm_override, int* iters,
+                        double* rel_out) {
+    const int n = B.n;
+    const int nb = gridDim.x;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gstride = gridDim.x * blockDim.x;
+    double* part = B.part;
+    double rz_p = 0.0, bb_p = 0.0;
+    for (int i = gtid; i < n; i += gstride) {
+        const double bi = rhs[i];
+        d[i] = 0.0;
+        B.r[i] = bi;
+        const double zi = B.dinv[i] * bi;
+        B.p[i] = zi;
+        rz_p += bi * zi;
+        bb_p += bi * bi;
+    }
+    rz_p = block_sum(rz_p, sh);
+    bb_p = block_sum(bb_p, sh);
+    if (threadIdx.x == 0) {
+        part[0 * nb + blockIdx.x] = rz_p;
+        part[1 * nb + blockIdx.x] = bb_p;
+    }
+    if (!grid_sync(gs)) return CUTCELL_E_BARRIER;
+    double rz = grid_reduce(part + 0 * nb, nb, sh);
+    double bnorm = sqrt(grid_reduce(part + 1 * nb, nb, sh));
+    if (rhs_norm_override > 0.0) bnorm = rhs_norm_override;
+    if (bnorm == 0.0) bnorm = 1.0;
+    int status = CUTCELL_E_NOCONV;
+    int k = 0;
+    double rel = 1.0;
+    for (k = 1; k <= maxiter; ++k) {
+        double pap = op.apply(B.p, B.Ap, gs, sm);
+        if (grid_error(gs)) return CUTCELL_E_BARRIER;
+        pap = block_sum(pap, sh);
+        if (threadIdx.x == 0) part[2 * nb + blockIdx.x] = pap;
+        if (!grid_sync(gs)) return CUTCELL_E_BARRIER;
+        pap = grid_reduce(part + 2 * nb, nb, sh);
+        if (!(pap > 0.0) || !isfinite(pap)) {
+            status = CUTCELL_E_BREAKDOWN;
+            break;
+        }
+        const double alpha = rz / pap;
+        double rr_p = 0.0, rzn_p = 0.0;
+        for (int i = gtid; i < n; i += gstride) {
+            const double pi = B.p[i];
+            d[i] += alpha * pi;
+            const double ri = B.r[i] - alpha * __ldcg(B.Ap + i);
+            B.r[i] = ri;
+            rr_p += ri * ri;
+            rzn_p += ri * (B.dinv[i] * ri);
+        }
+        rr_p = block_sum(rr_p, sh);
+        rzn_p = block_sum(rzn_p, sh);
+        if (threadIdx.x == 0) {
+            part[3 * nb + blockIdx.x] = rr_p;
+            part[4 * nb + blockIdx.x] = rzn_p;
+        }
+        if (!grid_sync(gs)) return CUTCELL_E_BARRIER;
+        const double rr = grid_reduce(part + 3 * nb, nb, sh);
+        const double rzn = grid_reduce(part + 4 * nb, nb, sh);
+        rel = sqrt(rr) / bnorm;
+        if (!isfinite(rel)) {
+            status = CUTCELL_E_NAN;
+            break;
+        }
+        if (rel <= tol) {
+            status = CUTCELL_OK;
+            break;
+        }
+        const double beta = rzn / rz;
+        rz = rzn;
+        for (int i = gtid; i < n; i += gstride) B.p[i] = B.dinv[i] * B.r[i] + beta * B.p[i];
+        if (!grid_sync(gs)) return CUTCELL_E_BARRIER;
+    }
+    *iters = (k > maxiter) ? maxiter : k;
+    *rel_out = rel;
+    return status;
+}
+
+// ||b - A x|| / ||b|| with the FP64 operator (overwrites Ap).
+template <class Op>
+__device__ double true_residual(const Op& op, const PcgBufs& B, const double* b, const double* x, double bnorm,
+                                const GridSync& gs, double* sm, double* sh, double* resid_out) {
+    const int nb = gridDim.x;
+    op.apply(x, B.Ap, gs, sm);
+    if (!grid_sync(gs)) return -1.0;
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += gridDim.x * blockDim.x) {
+        const double ri = b[i] - __ldcg(B.Ap + i);
+        if (resid_out) resid_out[i] = ri;
+        s += ri * ri;
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) B.part[5 * nb + blockIdx.x] = s;
+    if (!grid_sync(gs)) return -1.0;
+    return sqrt(grid_reduce(B.part + 5 * nb, nb, sh)) / bnorm;
+}
+
+__device__ __forceinline__ double norm_of(const double* v, int n, double* part, const GridSync& gs, double* sh,
+                                          int slot) {
+    const int nb = gridDim.x;
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += v[i] * v[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) part[slot * nb + blockIdx.x] = s;
+    if (!grid_sync(gs)) return -1.0;
+    return sqrt(grid_reduce(part + slot * nb, nb, sh));
+}
+
+struct SolveArgs {
+    const double* b;
+    double* x;
+    double tol;
+    int maxiter;
+    // refinement
+    double inner_tol;
+    int inner_maxiter;
+    int max_outer;
+    double* d;      // correction
+    double* rhat;   // outer residual
+    GridSync gs;
+    PcgBufs B;
+    DevResult* res;
+};
+
+// Plain FP64 PCG (the default form).
+template <class Op>
+__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) pcg_kernel(Op op, SolveArgs a) {
+    extern __shared__ double sm[];
+    __shared__ double sh[CUTCELL_WARPS + 1];
+    int iters = 0;
+    double rel = 1.0;
+    int status = pcg_core(op, a.B, a.b, a.x, a.tol, a.maxiter, a.gs, sm, sh, -1.0, &iters, &rel);
+    double true_rel = -1.0;
+    if (status != CUTCELL_E_BARRIER && !grid_error(a.gs)) {
+        const double bn = norm_of(a.b, a.B.n, a.B.part, a.gs, sh, 6);
+        true_rel = true_residual(op, a.B, a.b, a.x, bn == 0.0 ? 1.0 : bn, a.gs, sm, sh, nullptr);
+    }
+    if (grid_error(a.gs)) status = CUTCELL_E_BARRIER;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.res->status = status;
+        a.res->iterations = iters;
+        a.res->outer = 1;
+        a.res->rel = rel;
+        a.res->true_rel = true_rel;
+    }
+}
+
+// FP64 iterative refinement around a reduced-precision inner PCG:
+//   x = 0; rhat = b
+//   repeat: solve A_lo d = rhat (PCG, relative tolerance inner_tol);
+//           x += d; rhat = b - A_64 x (FP64); stop when ||rhat||/||b|| <= tol.
+template <class OpHi, class OpLo>
+__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) ir_kernel(OpHi hi, OpLo lo, SolveArgs a) {
+    extern __shared__ double sm[];
+    __shared__ double sh[CUTCELL_WARPS + 1];
+    const int n = a.B.n;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gstride = gridDim.x * blockDim.x;
+    for (int i = gtid; i < n; i += gstride) {
+        a.x[i] = 0.0;
+        a.rhat[i] = a.b[i];
+    }
+    double bn = norm_of(a.b, n, a.B.part, a.gs, sh, 6);
+    if (bn == 0.0) bn = 1.0;
+    int total = 0, outer = 0;
+    int status = CUTCELL_E_NOCONV;
+    double true_rel = 1.0, rel_in = 1.0;
+    for (outer = 1; outer <= a.max_outer; ++outer) {
+        int it = 0;
+        const int budget = a.maxiter - total;
+        if (budget <= 0) break;
+        int st = pcg_core(lo, a.B, a.rhat, a.d, a.inner_tol, budget < a.inner_maxiter ? budget : a.inner_maxiter,
+                          a.gs, sm, sh, -1.0, &it, &rel_in);
+        total += it;
+        if (st == CUTCELL_E_BARRIER) {
+            status = st;
+            break;
+        }
+        for (int i = gtid; i < n; i += gstride) a.x[i] += a.d[i];
+        if (!grid_sync(a.gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        true_rel = true_residual(hi, a.B, a.b, a.x, bn, a.gs, sm, sh, a.rhat);
+        if (grid_error(a.gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        if (!isfinite(true_rel)) {
+            status = CUTCELL_E_NAN;
+            break;
+        }
+        if (true_rel <= a.tol) {
+            status = CUTCELL_OK;
+            break;
+        }
+        if (st == CUTCELL_E_BREAKDOWN && it <= 1) {
+            status = st;
+            break;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.res->status = status;
+        a.res->iterations = total;
+        a.res->outer = outer > a.max_outer ? a.max_outer : outer;
+        a.res->rel = true_rel;
+        a.res->true_rel = true_rel;
+    }
+}
+
+// Single apply (operator benchmarks and tests): y = A x.
+template <class Op>
+__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) apply_kernel(Op op, const double* x, double* y, GridSync gs) {
+    extern __shared__ double sm[];
+    op.apply(x, y, gs, sm);
+}

@@ -1,0 +1,148 @@
+"""ctypes binding of libcutcell_b200.so (the C ABI declared in include/cutcell_b200.h).
+
+The library is built in-tree by ``cutcell_b200.build`` (nvcc, sm_100a).  There
+is no fallback: if the shared object is missing or cannot be loaded, every
+entry point raises ``CutcellLibraryError``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_NAME = "libcutcell_b200.so"
+LIB_PATH = Path(__file__).resolve().parent / LIB_NAME
+
+OK = 0
+E_NOCONV = 1
+E_BREAKDOWN = 2
+E_NAN = 3
+E_SHAPE = 4
+E_CUDA = 5
+E_BARRIER = 6
+E_ARG = 7
+
+FP64 = 0
+FP32_IR = 1
+BF16_IR = 2
+PRECISIONS = {"fp64": FP64, "fp32-ir": FP32_IR, "bf16-ir": BF16_IR}
+
+PRECOND_NONE = 0
+PRECOND_JACOBI = 1
+PRECOND_JACOBI_LEARNED = 2
+
+
+class CutcellLibraryError(RuntimeError):
+    pass
+
+
+class CutcellReport(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("iterations", C.c_int32),
+        ("outer_iterations", C.c_int32),
+        ("blocks", C.c_int32),
+        ("relative_residual", C.c_double),
+        ("true_relative_residual", C.c_double),
+        ("elapsed_ms", C.c_double),
+    ]
+
+
+_P = C.c_void_p
+
+
+class CutcellTileDesc(C.Structure):
+    _fields_ = [
+        ("n_elements", C.c_int32),
+        ("degree", C.c_int32),
+        ("tile", C.c_int32),
+        ("n_tiles_axis", C.c_int32),
+        ("n_tile_list", C.c_int32),
+        ("n_cut", C.c_int32),
+        ("n_full", C.c_int32),
+        ("n_red", C.c_int32),
+        ("n_small", C.c_int32),
+        ("a_mass", C.c_double),
+        ("tile_list", _P),
+        ("tile_kind", _P),
+        ("tile_eptr", _P),
+        ("tile_elem", _P),
+        ("tile_ecut", _P),
+        ("M1", _P),
+        ("Kt1", _P),
+        ("TM", _P),
+        ("TA", _P),
+        ("TK", _P),
+        ("cut_mats", _P),
+        ("red_of_full", _P),
+        ("small_slot", _P),
+        ("small_ptr", _P),
+        ("small_idx", _P),
+        ("small_val", _P),
+        ("full_of_red", _P),
+        ("smallT_ptr", _P),
+        ("smallT_row", _P),
+        ("smallT_val", _P),
+        ("diag", _P),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/cutcell_b200.h
+SIGNATURES = {
+    "cutcell_pcg_create_csr": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, C.POINTER(_P)]),
+    "cutcell_pcg_create_tiles": (C.c_int, [C.POINTER(CutcellTileDesc), C.POINTER(_P)]),
+    "cutcell_set_refinement": (C.c_int, [_P, C.c_double, C.c_int32, C.c_int32]),
+    "cutcell_pcg_solve": (
+        C.c_int,
+        [_P, _P, _P, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.POINTER(CutcellReport), _P],
+    ),
+    "cutcell_apply": (C.c_int, [_P, _P, _P, C.c_int32, _P]),
+    "cutcell_ext_gather": (C.c_int, [_P, _P, _P, _P]),
+    "cutcell_ext_scatter": (C.c_int, [_P, _P, _P, _P]),
+    "cutcell_destroy": (C.c_int, [_P]),
+    "cutcell_status_string": (C.c_char_p, [C.c_int]),
+    "cutcell_last_error": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the in-tree shared library (raises if it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("CUTCELL_B200_LIB", LIB_PATH))
+    if not path.exists():
+        raise CutcellLibraryError(
+            f"{path} is missing: build it with `python -m cutcell_b200.build` (nvcc, sm_100a)"
+        )
+    try:
+        lib = C.CDLL(str(path))
+    except OSError as exc:  # pragma: no cover - depends on the CUDA runtime
+        raise CutcellLibraryError(f"cannot load {path}: {exc}") from exc
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int, what: str) -> None:
+    if status != OK:
+        lib = load()
+        msg = lib.cutcell_status_string(status).decode()
+        extra = lib.cutcell_last_error().decode()
+        raise CutcellLibraryError(f"{what} failed: {msg}" + (f" ({extra})" if extra else ""))
+
+
+def status_message(status: int) -> str:
+    return load().cutcell_status_string(int(status)).decode()
+
+
+def current_stream_ptr() -> int:
+    import torch
+
+    return int(torch.cuda.current_stream().cuda_stream)

@@ -1,0 +1,174 @@
+"""Polynomial-preserving aggregation (extension) ``E`` for 3D cut-cell spaces.
+
+Same construction as ``polynomial_preserving_extension_3d``
+(code/bell_3d_core.py:471-542): coordinates with fluid-mass ratio
+``gamma >= 0.04`` are interior and map to themselves; every other active
+coordinate gets the least-squares weights that reproduce all total-degree
+``<= p`` monomials (spline coefficients by Greville interpolation,
+code/bell_3d_core.py:444-458) from its nearest interior Greville neighbours,
+starting from ``n_terms + 8`` and growing by 8 while the moment matrix is rank
+deficient (``matrix_rank(tol=1e-10)``), at most ``6 n_terms``; weights with
+``|w| <= 1e-14`` are dropped.  The neighbour ordering uses the same
+``argsort`` of Euclidean Greville distances, evaluated in row chunks so the
+distance matrix never has to be materialised whole (each row's ordering is
+independent of the others, so chunking changes no index).
+
+Besides the CSR matrix this module emits the device layout the gather/scatter
+kernels consume: an int32 map ``red_of_full`` for the identity rows, a CSR of
+the small rows, and the transposed CSR of the small rows (sorted by full
+index) so ``E^T`` needs no atomics.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import scipy.sparse as sp
+
+from .bspline import OpenUniformBasis, polynomial_coefficients
+
+
+@dataclass
+class Extension:
+    E: sp.csr_matrix
+    interior: np.ndarray
+    small_support: np.ndarray
+    active: np.ndarray
+    gamma: np.ndarray
+    polynomial_residual: float
+
+    @property
+    def n_full(self) -> int:
+        return self.E.shape[0]
+
+    @property
+    def n_red(self) -> int:
+        return self.E.shape[1]
+
+    def device_layout(self) -> dict:
+        """Index maps for the E gather / E^T scatter kernels (int32, fp64)."""
+        n_full, n_red = self.E.shape
+        red_of_full = np.full(n_full, -1, dtype=np.int32)
+        red_of_full[self.interior] = np.arange(n_red, dtype=np.int32)
+        small = np.asarray(self.small_support, dtype=np.int64)
+        Es = self.E[small].tocsr()
+        Es.sort_indices()
+        small_slot = np.full(n_full, -1, dtype=np.int32)
+        small_slot[small] = np.arange(small.size, dtype=np.int32)
+        # transposed small rows: for reduced column j, entries (full row b, weight)
+        EsT = sp.csr_matrix(
+            (Es.data, Es.indices, Es.indptr), shape=(small.size, n_red)
+        ).T.tocsr()
+        EsT.sort_indices()
+        return {
+            "red_of_full": red_of_full,
+            "full_of_red": np.asarray(self.interior, dtype=np.int32),
+            "small_rows": small.astype(np.int32),
+            "small_slot": small_slot,
+            "small_ptr": Es.indptr.astype(np.int32),
+            "small_idx": Es.indices.astype(np.int32),
+            "small_val": Es.data.astype(np.float64),
+            "smallT_ptr": EsT.indptr.astype(np.int32),
+            # column of EsT is the slot in small_rows -> convert to full index
+            "smallT_row": small[EsT.indices].astype(np.int32),
+            "smallT_val": EsT.data.astype(np.float64),
+        }
+
+
+def greville_3d(basis: OpenUniformBasis) -> np.ndarray:
+    g = basis.greville
+    nb = basis.n_basis
+    X = np.tile(np.tile(g, nb), nb)
+    Y = np.tile(np.repeat(g, nb), nb)
+    Z = np.repeat(g, nb * nb)
+    return np.column_stack([X, Y, Z])
+
+
+def monomial_rows_3d(basis: OpenUniformBasis, degree: int) -> np.ndarray:
+    c = polynomial_coefficients(basis, degree)
+    rows = []
+    for total in range(degree + 1):
+        for a in range(total + 1):
+            for b in range(total - a + 1):
+                cc = total - a - b
+                rows.append(np.einsum("k,j,i->kji", c[cc], c[b], c[a]).reshape(-1))
+    return np.vstack(rows)
+
+
+def build_extension(
+    gamma: np.ndarray,
+    basis: OpenUniformBasis,
+    degree: int,
+    *,
+    support_threshold: float = 0.04,
+    preserve_degree: int | None = None,
+    mass_diag: np.ndarray | None = None,
+    chunk: int = 64,
+) -> Extension:
+    deg = degree if preserve_degree is None else int(preserve_degree)
+    gamma = np.asarray(gamma, dtype=float)
+    active = np.where(gamma > 0.0)[0]
+    interior = np.where(gamma >= support_threshold)[0]
+    small = np.array([i for i in active if gamma[i] < support_threshold], dtype=int)
+    if interior.size == 0:
+        raise ValueError("no interior coordinates")
+    n_full = gamma.size
+    greville = greville_3d(basis)
+    col = np.full(n_full, -1, dtype=np.int64)
+    col[interior] = np.arange(interior.size)
+    rows_t = [interior.astype(np.int64)]
+    cols_t = [np.arange(interior.size, dtype=np.int64)]
+    vals_t = [np.ones(interior.size)]
+
+    if deg == 0:
+        # constants only: mass-weighted average of the 8 nearest interior
+        # neighbours (code/bell_3d_core.py:496-511)
+        m_diag = np.asarray(mass_diag if mass_diag is not None else np.ones(n_full))
+        for b in small:
+            dist = np.linalg.norm(greville[interior] - greville[int(b)], axis=1)
+            nb = interior[np.argsort(dist)[:8]]
+            w = np.maximum(m_diag[nb], 0.0)
+            w = w / max(float(w.sum()), 1.0e-300)
+            rows_t.append(np.full(nb.size, int(b)))
+            cols_t.append(col[nb])
+            vals_t.append(w)
+        E = sp.csr_matrix(
+            (np.concatenate(vals_t), (np.concatenate(rows_t), np.concatenate(cols_t))),
+            shape=(n_full, interior.size),
+        )
+        E.sort_indices()
+        return Extension(E, interior, small, active, gamma, 0.0)
+
+    poly = monomial_rows_3d(basis, deg)
+    n_terms = poly.shape[0]
+    gi = greville[interior]
+    for s0 in range(0, small.size, chunk):
+        blk = small[s0 : s0 + chunk]
+        order = np.argsort(np.linalg.norm(gi[None, :, :] - greville[blk][:, None, :], axis=2), axis=1)
+        for r, b in enumerate(blk):
+            ordered = interior[order[r]]
+            k = n_terms
+            chosen = ordered[: k + 8]
+            C = poly[:, chosen]
+            while np.linalg.matrix_rank(C, tol=1.0e-10) < n_terms and len(chosen) < min(
+                len(ordered), 6 * n_terms
+            ):
+                k += 8
+                chosen = ordered[: k + 8]
+                C = poly[:, chosen]
+            w, *_ = np.linalg.lstsq(C, poly[:, int(b)], rcond=None)
+            keep = np.abs(w) > 1.0e-14
+            rows_t.append(np.full(int(keep.sum()), int(b)))
+            cols_t.append(col[chosen[keep]])
+            vals_t.append(w[keep])
+    E = sp.csr_matrix(
+        (np.concatenate(vals_t), (np.concatenate(rows_t), np.concatenate(cols_t))),
+        shape=(n_full, interior.size),
+    )
+    E.sort_indices()
+    active_mask = (gamma > 0.0).astype(float)
+    res = 0.0
+    for row in poly:
+        res = max(res, float(np.max(np.abs(E @ row[interior] - row * active_mask))))
+    return Extension(E, interior, small, active, gamma, res)

@@ -1,0 +1,57 @@
+"""Build recipe for libcutcell_b200.so (in-tree, sm_100a).
+
+    python -m cutcell_b200.build          # from gpu-cutcell-navier-stokes_b200/
+
+nvcc cross-compiles without a GPU; the .so lands next to this file so it
+travels with the source tree.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = ROOT / "csrc"
+SOURCES = ["cutcell.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    out = PKG / "libcutcell_b200.so"
+    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [ROOT.parent / "include" / "cutcell_b200.h"]
+    if out.exists() and not force and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps if d.exists()):
+        return out
+    cmd = [
+        nvcc(),
+        *ARCH,
+        "-lineinfo",
+        "-O3",
+        "-std=c++17",
+        "-Xcompiler",
+        "-fPIC",
+        "-shared",
+        *(["-Xptxas", "-v"] if verbose else []),
+        *[str(CSRC / s) for s in SOURCES],
+        "-o",
+        str(out) + ".tmp",
+    ]
+    subprocess.run(cmd, check=True, cwd=str(ROOT))
+    os.replace(str(out) + ".tmp", out)
+    return out
+
+
+if __name__ == "__main__":
+    p = build(verbose="-v" in sys.argv, force="--force" in sys.argv)
+    print(p)

@@ -1,0 +1,120 @@
+"""Named synthetic workloads (seeded, no external data).
+
+* ``sphere_poisson``: Poisson on [0,1]^3 minus the ball |x - (1/2,1/2,1/2)| < r,
+  weak-penalty Dirichlet data u = sin(pi x) sin(pi y) sin(pi z) on the sphere
+  and the box faces, p = 3, n elements per axis (the learned-preconditioner
+  problem: r = 0.31, n = 32).
+* ``plane_poisson``: the same PDE on the unit box cut by a plane whose normal
+  is rotated 5 degrees from the x axis, offset chosen so the worst cut cell has
+  the requested fluid fraction (p = 3, n = 8 by default).
+
+Problems are cached as .npz (keyed by their parameters) so repeated runs in
+one session skip the host setup.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import os
+from pathlib import Path
+
+import numpy as np
+
+from .aggregation import build_extension
+from .cutgeom import PlaneLevelSet, SphereExteriorLevelSet
+from .problem import CutCellProblem, build_problem, manufactured_sine
+
+_CACHE = Path(os.environ.get("CUTCELL_CACHE", Path.home() / ".cache" / "cutcell_b200"))
+_FIELDS = ["elem_type", "M1", "Kt1", "cut_ids", "cut_mats", "h_cut_diag", "h_bg_diag", "load", "cut_fractions"]
+
+
+def _key(**kw) -> str:
+    s = repr(sorted(kw.items()))
+    return hashlib.sha1(s.encode()).hexdigest()[:16]
+
+
+def _cached(key: str, builder) -> CutCellProblem:
+    path = _CACHE / f"{key}.npz"
+    if path.exists():
+        try:
+            z = np.load(path, allow_pickle=False)
+            from .bspline import make_basis
+
+            meta = z["meta"]
+            n, p = int(meta[0]), int(meta[1])
+            return CutCellProblem(
+                n_elements=n, degree=p, basis=make_basis(n, p), a_mass=float(meta[2]), a_stiff=float(meta[3]),
+                nitsche=bool(meta[4]), beta=float(meta[5]), **{k: z[k] for k in _FIELDS},
+            )
+        except Exception:
+            pass
+    prob = builder()
+    try:
+        _CACHE.mkdir(parents=True, exist_ok=True)
+        meta = np.array([prob.n_elements, prob.degree, prob.a_mass, prob.a_stiff, float(prob.nitsche), prob.beta])
+        np.savez(str(path) + ".tmp.npz", meta=meta, **{k: getattr(prob, k) for k in _FIELDS})
+        os.replace(str(path) + ".tmp.npz", path)
+    except OSError:
+        pass
+    return prob
+
+
+def sphere_poisson(n: int = 32, p: int = 3, radius: float = 0.31, a_mass: float = 0.0, cache: bool = True):
+    u, f = manufactured_sine()
+    phi = SphereExteriorLevelSet((0.5, 0.5, 0.5), radius)
+    build = lambda: build_problem(phi, n, p, a_mass=a_mass, forcing=f, dirichlet=u)
+    prob = _cached(_key(kind="sphere", n=n, p=p, r=radius, a=a_mass, v=2), build) if cache else build()
+    ext = build_extension(prob.gamma, prob.basis, p)
+    return prob, ext
+
+
+def plane_offset_for_fraction(n: int, angle_deg: float, fraction: float) -> float:
+    """Offset of the plane n.x = c such that the smallest nonzero cut-cell
+    fluid fraction equals ``fraction`` (bisection on the exact polyhedral
+    volumes of the cut cells)."""
+    a = np.deg2rad(angle_deg)
+    normal = (np.cos(a), np.sin(a), 0.0)
+    h = 1.0 / n
+
+    def worst(c):
+        from .cutgeom import cut_cell_quadrature
+
+        phi = PlaneLevelSet(normal, c)
+        fr = []
+        for iy in range(n):
+            for ix in range(n):
+                lo = np.array([ix * h, iy * h, 0.0])
+                C = lo[None, :] + h * np.array([[i & 1, (i >> 1) & 1, (i >> 2) & 1] for i in range(8)], dtype=float)
+                f = phi(C[:, 0], C[:, 1], C[:, 2])
+                if f.min() < 0 < f.max():
+                    fr.append(cut_cell_quadrature(phi, lo, h, 1, box_faces=False).volume / h**3)
+        return min(fr) if fr else 1.0
+
+    # search c in the first layer of cells along x where the smallest slivers live
+    lo, hi = 0.5 * h, 1.5 * h
+    wl, wh = worst(lo), worst(hi)
+    best = lo
+    for _ in range(60):
+        mid = 0.5 * (lo + hi)
+        wm = worst(mid)
+        best = mid
+        if abs(wm - fraction) < 1e-12:
+            break
+        # the worst fraction is not monotone in c in general; keep the side
+        # whose end value brackets the target
+        if (wl - fraction) * (wm - fraction) <= 0:
+            hi, wh = mid, wm
+        else:
+            lo, wl = mid, wm
+    return best
+
+
+def plane_poisson(n: int = 8, p: int = 3, angle_deg: float = 5.0, fraction: float = 0.15, cache: bool = True):
+    u, f = manufactured_sine()
+    c = plane_offset_for_fraction(n, angle_deg, fraction)
+    a = np.deg2rad(angle_deg)
+    phi = PlaneLevelSet((np.cos(a), np.sin(a), 0.0), c)
+    build = lambda: build_problem(phi, n, p, forcing=f, dirichlet=u)
+    prob = _cached(_key(kind="plane", n=n, p=p, ang=angle_deg, fr=fraction, v=2), build) if cache else build()
+    ext = build_extension(prob.gamma, prob.basis, p)
+    return prob, ext, c

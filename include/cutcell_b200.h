@@ -1,0 +1,137 @@
+/*
+ * cutcell_b200.h -- C ABI of libcutcell_b200.so, the B200 (sm_100a) solve path
+ * for aggregated cut-cell systems.
+ *
+ * Conventions for every entry point:
+ *   - all array pointers are DEVICE pointers (e.g. torch.Tensor.data_ptr());
+ *   - the caller keeps its arrays alive for the lifetime of a context that
+ *     references them; contexts own only their device scratch and free it in
+ *     cutcell_destroy;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream);
+ *   - every call returns a status code (CUTCELL_OK = 0); solver outcomes that
+ *     the reference reports as success=False ("maximum iterations reached",
+ *     "CG breakdown: non-positive curvature") come back as a status code and a
+ *     filled report, never as a crash, and there is no CPU fallback.
+ *
+ * Index layout: DOFs are flattened x-fastest, (iz*ny + iy)*nx + ix
+ * (code/cut_3d_sbp.py:20-22, code/bell_3d_core.py:313-317).
+ */
+#ifndef CUTCELL_B200_H
+#define CUTCELL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CUTCELL_OK = 0,
+    CUTCELL_E_NOCONV = 1,     /* maxiter reached: "maximum iterations reached" */
+    CUTCELL_E_BREAKDOWN = 2,  /* p.Ap <= 0 or non-finite: "CG breakdown: non-positive curvature" */
+    CUTCELL_E_NAN = 3,        /* non-finite residual */
+    CUTCELL_E_SHAPE = 4,      /* inconsistent sizes / layout */
+    CUTCELL_E_CUDA = 5,       /* a CUDA runtime call failed */
+    CUTCELL_E_BARRIER = 6,    /* a bounded device-wide wait ran out */
+    CUTCELL_E_ARG = 7         /* invalid argument */
+};
+
+enum { CUTCELL_FP64 = 0, CUTCELL_FP32_IR = 1, CUTCELL_BF16_IR = 2 };
+enum { CUTCELL_PRECOND_NONE = 0, CUTCELL_PRECOND_JACOBI = 1, CUTCELL_PRECOND_JACOBI_LEARNED = 2 };
+
+typedef struct cutcell_ctx cutcell_ctx;
+
+/* Mirrors SolverReport (code/fast_solver_backends.py:30-45) for the device
+ * part: iterations counts the iteration in which the stopping test passed
+ * (code/fast_solver_backends.py:249-266); relative_residual is the recursive
+ * ||r||/||b||; true_relative_residual is ||b - A x||/||b|| recomputed in FP64
+ * on the device (b = 0 -> denominator 1, code/fast_solver_backends.py:63-71). */
+typedef struct {
+    int32_t status;
+    int32_t iterations;        /* total inner PCG iterations */
+    int32_t outer_iterations;  /* refinement sweeps (1 for plain FP64) */
+    int32_t blocks;            /* persistent grid size used */
+    double relative_residual;
+    double true_relative_residual;
+    double elapsed_ms;         /* device time of the solve (CUDA events) */
+} CutcellReport;
+
+/* Matrix-free operator description (host struct holding device pointers).
+ * Element blocks: full elements use per-axis 1D factors
+ *   Mz (x) My (x) (a_mass Mx + Kx) + Mz (x) Ky (x) Mx + Kz (x) My (x) Mx,
+ * cut elements a dense (p+1)^3 x (p+1)^3 block.  Tiles group tile^3 elements. */
+typedef struct {
+    int32_t n_elements;    /* per axis */
+    int32_t degree;
+    int32_t tile;          /* elements per tile edge */
+    int32_t n_tiles_axis;
+    int32_t n_tile_list;   /* number of nonempty tiles */
+    int32_t n_cut;
+    int32_t n_full;        /* (n_elements+degree)^3 */
+    int32_t n_red;
+    int32_t n_small;
+    double a_mass;
+    const int32_t* tile_list;  /* [n_tile_list] linear tile ids */
+    const int32_t* tile_kind;  /* [n_tiles_axis^3] 0 empty, 1 full, 2 mixed */
+    const int32_t* tile_eptr;  /* [n_tiles_axis^3 + 1] */
+    const int32_t* tile_elem;  /* local element id (ez*tile+ey)*tile+ex */
+    const int32_t* tile_ecut;  /* cut block index or -1 */
+    const double* M1;          /* [n][(p+1)^2] */
+    const double* Kt1;         /* [3][n][(p+1)^2] */
+    const double* TM;          /* [n_tiles_axis][D^2], D = tile+degree */
+    const double* TA;          /* [n_tiles_axis][D^2] */
+    const double* TK;          /* [3][n_tiles_axis][D^2] */
+    const double* cut_mats;    /* [n_cut][(p+1)^6] */
+    const int32_t* red_of_full;
+    const int32_t* small_slot;
+    const int32_t* small_ptr;
+    const int32_t* small_idx;
+    const double* small_val;
+    const int32_t* full_of_red;
+    const int32_t* smallT_ptr;
+    const int32_t* smallT_row;
+    const double* smallT_val;
+    const double* diag;        /* [n_red] diagonal of E^T A E (Jacobi) */
+} CutcellTileDesc;
+
+/* Replaces the CuPy CSR upload + Jacobi-CG loop of solve_gpu_cg
+ * (code/fast_solver_backends.py:194-289): CSR of the reduced SPD matrix
+ * (int32 indptr/indices, fp64 data), already on the device. */
+int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const int32_t* indices,
+                           const double* data, cutcell_ctx** out);
+
+/* Structured entry for the matrix-free E^T A E (the operator restrict_spd of
+ * code/bell_3d_core.py:550-552 forms explicitly). */
+int cutcell_pcg_create_tiles(const CutcellTileDesc* desc, cutcell_ctx** out);
+
+/* Refinement controls for the FP32/BF16 forms: inner relative tolerance,
+ * inner iteration cap per sweep, maximum sweeps. */
+int cutcell_set_refinement(cutcell_ctx* ctx, double inner_tol, int32_t inner_maxiter, int32_t max_outer);
+
+/* Jacobi-PCG from x = 0 to ||r||/||b|| <= tol; the same algorithm as
+ * solve_gpu_cg (code/fast_solver_backends.py:236-274), run as one persistent
+ * cooperative launch with no host round trip per iteration. precision is
+ * CUTCELL_FP64 (plain) or an iterative-refinement form; precond is
+ * CUTCELL_PRECOND_NONE or CUTCELL_PRECOND_JACOBI.  Blocks until done. */
+int cutcell_pcg_solve(cutcell_ctx* ctx, const double* b, double* x, double tol, int32_t maxiter,
+                      int32_t precision, int32_t precond, CutcellReport* report, void* stream);
+
+/* y = E^T A E x (reduced vectors), operator data in the given precision. */
+int cutcell_apply(cutcell_ctx* ctx, const double* x, double* y, int32_t precision, void* stream);
+
+/* Extension gather x_full = E x_red and transpose scatter y_red = E^T y_full
+ * (E as produced by polynomial_preserving_extension_3d,
+ * code/bell_3d_core.py:471-542); uses the tile descriptor's E arrays. */
+int cutcell_ext_gather(cutcell_ctx* ctx, const double* x_red, double* x_full, void* stream);
+int cutcell_ext_scatter(cutcell_ctx* ctx, const double* y_full, double* y_red, void* stream);
+
+int cutcell_destroy(cutcell_ctx* ctx);
+const char* cutcell_status_string(int status);
+/* Last CUDA error text seen by the library (diagnostics). */
+const char* cutcell_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUTCELL_B200_H */
