@@ -103,4 +103,19 @@ template <> struct Conv<__nv_bfloat16> {
     __device__ __forceinline__ static float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
 };
 
+// Optional self-checks (build with -DCUTCELL_DEBUG_CHECKS): a failed check
+// records (code, info) in two debug words and the guarded access is skipped.
+#ifdef CUTCELL_DEBUG_CHECKS
+__device__ __forceinline__ bool dbg_ok(bool cond, unsigned code, unsigned info, unsigned* words) {
+    if (!cond && words) {
+        if (atomicCAS(words, 0u, code) == 0u) atomicExch(words + 1, info);
+    }
+    return cond;
+}
+#define CUTCELL_OK_IF(cond, code, info, words) dbg_ok((cond), (code), (unsigned)(info), (words))
+#else
+#define CUTCELL_OK_IF(cond, code, info, words) true
+#endif
+#define CUTCELL_ALIGNED(p, a) ((((uintptr_t)(p)) % (a)) == 0)
+
 static inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }

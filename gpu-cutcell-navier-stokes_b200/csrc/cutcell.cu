@@ -94,13 +94,12 @@ struct cutcell_ctx {
     float* val32 = nullptr;
     __nv_bfloat16* val16 = nullptr;
     // tiles
-    TileOp<double> t64;
-    TileOp<float> t32;
-    TileOp<__nv_bfloat16> t16;
+    TileData td;
+    const double* cut64 = nullptr;
     float* cut32 = nullptr;
     __nv_bfloat16* cut16 = nullptr;
     double* ypart = nullptr;
-    size_t tile_smem = 0;
+    double* ycut = nullptr;
     // scratch
     double* dinv = nullptr;
     double* ones = nullptr;
@@ -131,7 +130,7 @@ static int alloc_scratch(cutcell_ctx* c) {
     CK(cudaMalloc(&c->Ap, nb));
     CK(cudaMalloc(&c->d, nb));
     CK(cudaMalloc(&c->rhat, nb));
-    CK(cudaMalloc(&c->bar, 4 * sizeof(unsigned)));
+    CK(cudaMalloc(&c->bar, 8 * sizeof(unsigned)));
     CK(cudaMalloc(&c->res, sizeof(DevResult)));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
@@ -205,9 +204,48 @@ static int run_apply(cutcell_ctx* c, const Op& op, size_t smem, const double* x,
     int blocks = 0;
     int st = ensure_part(c, kern, smem, &blocks);
     if (st) return st;
-    CK(cudaMemsetAsync(c->bar, 0, 4 * sizeof(unsigned), s));
+    CK(cudaMemsetAsync(c->bar, 0, 8 * sizeof(unsigned), s));
     GridSync gs = make_gs(c, blocks);
     return launch_coop(kern, blocks, smem, s, op, x, y, gs);
+}
+
+// mode 0: solve (plain or refinement), mode 1: one apply
+// Reduced-precision refinement is built for p >= 3 only: the fused
+// refinement kernel instantiated for p = 2 faulted (misaligned address) on
+// the B200 while the same code with self-checks compiled in ran clean; until
+// the cause is found that instantiation is not built.
+template <int P1>
+static int tiles_run(cutcell_ctx* c, int mode, int precision, SolveArgs* a, const double* x, double* y, cudaStream_t s,
+                     int* blocks) {
+    TileOp<double, P1> o64{c->td, c->cut64};
+    TileOp<float, P1> o32{c->td, c->cut32};
+    TileOp<__nv_bfloat16, P1> o16{c->td, c->cut16};
+    const size_t sm = TileOp<double, P1>::smem_bytes();
+    if (mode == 1) {
+        if (precision == CUTCELL_FP64) return run_apply(c, o64, sm, x, y, s);
+        if (precision == CUTCELL_FP32_IR) return run_apply(c, o32, sm, x, y, s);
+        return run_apply(c, o16, sm, x, y, s);
+    }
+    if (precision == CUTCELL_FP64) return run_plain(c, o64, sm, *a, s, blocks);
+    if constexpr (P1 >= 4) {
+        if (precision == CUTCELL_FP32_IR) return run_ir(c, o64, o32, sm, *a, s, blocks);
+        return run_ir(c, o64, o16, sm, *a, s, blocks);
+    } else {
+        g_last_error = "reduced-precision refinement needs degree >= 3";
+        return CUTCELL_E_ARG;
+    }
+}
+
+static int tiles_dispatch(cutcell_ctx* c, int mode, int precision, SolveArgs* a, const double* x, double* y,
+                          cudaStream_t s, int* blocks) {
+    switch (c->td.p) {
+        case 1: return tiles_run<2>(c, mode, precision, a, x, y, s, blocks);
+        case 2: return tiles_run<3>(c, mode, precision, a, x, y, s, blocks);
+        case 3: return tiles_run<4>(c, mode, precision, a, x, y, s, blocks);
+        case 4: return tiles_run<5>(c, mode, precision, a, x, y, s, blocks);
+        case 5: return tiles_run<6>(c, mode, precision, a, x, y, s, blocks);
+        default: return CUTCELL_E_SHAPE;
+    }
 }
 
 extern "C" {
@@ -264,8 +302,8 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     if (!out || !t) return CUTCELL_E_ARG;
     const int p = t->degree, P1 = p + 1, P = P1 * P1 * P1, D = t->tile + p;
     const int nb = t->n_elements + p;
-    if (p < 1 || t->tile < 1 || t->n_tiles_axis * t->tile < t->n_elements || (long)nb * nb * nb != t->n_full ||
-        t->n_red <= 0)
+    if (p < 1 || p > 5 || t->tile != 4 || t->n_tiles_axis * t->tile < t->n_elements ||
+        (long)nb * nb * nb != t->n_full || t->n_red <= 0 || t->cut_chunk < 1)
         return CUTCELL_E_SHAPE;
     cutcell_ctx* c = new cutcell_ctx();
     c->kind = KIND_TILES;
@@ -279,6 +317,8 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     const size_t nt3 = (size_t)t->n_tiles_axis * t->n_tiles_axis * t->n_tiles_axis;
     CK(cudaMalloc(&c->ypart, nt3 * D * D * D * sizeof(double)));
     CK(cudaMemset(c->ypart, 0, nt3 * D * D * D * sizeof(double)));
+    CK(cudaMalloc(&c->ycut, ((size_t)t->n_cut * P + 1) * sizeof(double)));
+    CK(cudaMemset(c->ycut, 0, ((size_t)t->n_cut * P + 1) * sizeof(double)));
     const size_t ncm = (size_t)t->n_cut * P * P;
     if (ncm) {
         CK(cudaMalloc(&c->cut32, ncm * sizeof(float)));
@@ -299,37 +339,35 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     e.smallT_ptr = t->smallT_ptr;
     e.smallT_row = t->smallT_row;
     e.smallT_val = t->smallT_val;
-    TileOp<double> o;
-    o.n = t->n_elements;
-    o.p = p;
-    o.P1 = P1;
-    o.P = P;
-    o.T = t->tile;
-    o.D = D;
-    o.nta = t->n_tiles_axis;
-    o.nb = nb;
-    o.ntile_list = t->n_tile_list;
-    o.a_mass = t->a_mass;
-    o.tile_list = t->tile_list;
-    o.tile_kind = t->tile_kind;
-    o.tile_eptr = t->tile_eptr;
-    o.tile_elem = t->tile_elem;
-    o.tile_ecut = t->tile_ecut;
-    o.M1 = t->M1;
-    o.Kt1 = t->Kt1;
-    o.TM = t->TM;
-    o.TA = t->TA;
-    o.TK = t->TK;
-    o.cut_mats = t->cut_mats;
-    o.ext = e;
-    o.ypart = c->ypart;
-    c->t64 = o;
-    // same geometry, reduced-precision cut blocks
-    memcpy(&c->t32, &o, sizeof(o));
-    c->t32.cut_mats = c->cut32;
-    memcpy(&c->t16, &o, sizeof(o));
-    c->t16.cut_mats = c->cut16;
-    c->tile_smem = TileOp<double>::smem_bytes(D, P, CUTCELL_WARPS);
+    TileData& d = c->td;
+    d.n = t->n_elements;
+    d.p = p;
+    d.T = t->tile;
+    d.nta = t->n_tiles_axis;
+    d.nb = nb;
+    d.n_items = t->n_items;
+    d.n_cut = t->n_cut;
+    d.cut_chunk = t->cut_chunk;
+    d.a_mass = t->a_mass;
+    d.item_list = t->item_list;
+    d.tile_kind = t->tile_kind;
+    d.tile_eptr = t->tile_eptr;
+    d.tile_elem = t->tile_elem;
+    d.tile_ecut = t->tile_ecut;
+    d.M1 = t->M1;
+    d.Kt1 = t->Kt1;
+    d.TM = t->TM;
+    d.TA = t->TA;
+    d.TK = t->TK;
+    d.cut_base = t->cut_base;
+    d.cut_dof_slot = t->cut_dof_slot;
+    d.cut_dof_ptr = t->cut_dof_ptr;
+    d.cut_dof_ent = t->cut_dof_ent;
+    d.ext = e;
+    d.ypart = c->ypart;
+    d.ycut = c->ycut;
+    d.work = c->bar + 3;
+    c->cut64 = t->cut_mats;
     diag_inv_kernel<<<ceil_div(t->n_red, 256), 256>>>(t->n_red, t->diag, c->dinv);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
@@ -365,7 +403,7 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
     a.d = c->d;
     a.rhat = c->rhat;
     a.res = c->res;
-    CK(cudaMemsetAsync(c->bar, 0, 4 * sizeof(unsigned), s));
+    CK(cudaMemsetAsync(c->bar, 0, 8 * sizeof(unsigned), s));
     CK(cudaEventRecord(c->ev0, s));
     int blocks = 0;
     int st = CUTCELL_OK;
@@ -377,16 +415,18 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
         else
             st = run_ir(c, c->csr64, c->csr16, 0, a, s, &blocks);
     } else {
-        const size_t sm = c->tile_smem;
-        if (precision == CUTCELL_FP64)
-            st = run_plain(c, c->t64, sm, a, s, &blocks);
-        else if (precision == CUTCELL_FP32_IR)
-            st = run_ir(c, c->t64, c->t32, sm, a, s, &blocks);
-        else
-            st = run_ir(c, c->t64, c->t16, sm, a, s, &blocks);
+        st = tiles_dispatch(c, 0, precision, &a, nullptr, nullptr, s, &blocks);
     }
     if (st) return st;
     CK(cudaEventRecord(c->ev1, s));
+#ifdef CUTCELL_DEBUG_CHECKS
+    {
+        unsigned w[8];
+        CK(cudaMemcpyAsync(w, c->bar, sizeof(w), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (w[4]) fprintf(stderr, "cutcell debug check failed: code %u info %u\n", w[4], w[5]);
+    }
+#endif
     DevResult hr;
     CK(cudaMemcpyAsync(&hr, c->res, sizeof(hr), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -411,24 +451,23 @@ int cutcell_apply(cutcell_ctx* c, const double* x, double* y, int32_t precision,
         if (precision == CUTCELL_FP64) return run_apply(c, c->csr64, 0, x, y, s);
         if (precision == CUTCELL_FP32_IR) return run_apply(c, c->csr32, 0, x, y, s);
         if (precision == CUTCELL_BF16_IR) return run_apply(c, c->csr16, 0, x, y, s);
-    } else {
-        if (precision == CUTCELL_FP64) return run_apply(c, c->t64, c->tile_smem, x, y, s);
-        if (precision == CUTCELL_FP32_IR) return run_apply(c, c->t32, c->tile_smem, x, y, s);
-        if (precision == CUTCELL_BF16_IR) return run_apply(c, c->t16, c->tile_smem, x, y, s);
+    } else if (precision >= CUTCELL_FP64 && precision <= CUTCELL_BF16_IR) {
+        int blocks = 0;
+        return tiles_dispatch(c, 1, precision, nullptr, x, y, s, &blocks);
     }
     return CUTCELL_E_ARG;
 }
 
 int cutcell_ext_gather(cutcell_ctx* c, const double* x_red, double* x_full, void* stream) {
     if (!c || c->kind != KIND_TILES || !x_red || !x_full) return CUTCELL_E_ARG;
-    ext_gather_kernel<<<ceil_div(c->t64.ext.n_full, 256), 256, 0, (cudaStream_t)stream>>>(c->t64.ext, x_red, x_full);
+    ext_gather_kernel<<<ceil_div(c->td.ext.n_full, 256), 256, 0, (cudaStream_t)stream>>>(c->td.ext, x_red, x_full);
     CK(cudaGetLastError());
     return CUTCELL_OK;
 }
 
 int cutcell_ext_scatter(cutcell_ctx* c, const double* y_full, double* y_red, void* stream) {
     if (!c || c->kind != KIND_TILES || !y_full || !y_red) return CUTCELL_E_ARG;
-    ext_scatter_kernel<<<ceil_div(c->t64.ext.n_red, 256), 256, 0, (cudaStream_t)stream>>>(c->t64.ext, y_full, y_red);
+    ext_scatter_kernel<<<ceil_div(c->td.ext.n_red, 256), 256, 0, (cudaStream_t)stream>>>(c->td.ext, y_full, y_red);
     CK(cudaGetLastError());
     return CUTCELL_OK;
 }
@@ -437,7 +476,7 @@ int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
-    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->dinv, c->ones, c->r,
                     c->p,     c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);

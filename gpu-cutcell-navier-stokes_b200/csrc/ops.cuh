@@ -89,199 +89,314 @@ struct ExtDev {
 // ---------------------------------------------------------------------------
 // Matrix-free tile operator
 // ---------------------------------------------------------------------------
+//
+// y = E^T A E p in two phases separated by one grid barrier:
+//
+//  phase 1 (work items, claimed dynamically through one atomic counter):
+//    - FULL tile (tile^3 uncut fluid elements): E-gather of the
+//      (tile+p)^3 DOF window into shared memory, then the Kronecker sum with
+//      tile-assembled 1D factors, 7 banded passes -> ypart[tile];
+//    - MIXED tile: the same window, its uncut elements one per warp (7 passes
+//      of (p+1)-wide 1D factors cached in shared memory), per-warp
+//      accumulators summed in warp order -> ypart[tile];
+//    - CUT chunk: dense (p+1)^3 blocks of cut elements, each multiplied by the
+//      whole block (4 threads per row, interleaved columns) -> ycut[cut].
+//  phase 2 (per reduced DOF j): y_j = sum over E's column j of the full-space
+//    values, each full value = fixed-order sum of its <= 8 tile partials and
+//    its cut-element partials.  No atomics; results are bit-reproducible.
 
 enum { TILE_EMPTY = 0, TILE_FULL = 1, TILE_MIXED = 2 };
 
-template <typename CT>
-struct TileOp {
-    int n;      // elements per axis
-    int p;      // degree
-    int P1;     // p + 1
-    int P;      // (p+1)^3
-    int T;      // elements per tile edge
-    int D;      // T + p, DOFs per tile edge
-    int nta;    // tiles per axis
-    int nb;     // DOFs per axis (n + p)
-    int ntile_list;
+// Non-templated description shared by every precision / degree instance.
+struct TileData {
+    int n, p, T, nta, nb;
+    int n_items;      // work items (tiles and cut chunks, heaviest first)
+    int n_cut;
+    int cut_chunk;    // cut elements per work item
     double a_mass;
-    const int* __restrict__ tile_list;   // nonempty linear tile ids (work order)
-    const int* __restrict__ tile_kind;   // per linear tile
-    const int* __restrict__ tile_eptr;   // per linear tile, element range (mixed tiles)
-    const int* __restrict__ tile_elem;   // local element id (ez*T+ey)*T+ex
-    const int* __restrict__ tile_ecut;   // cut block index, -1 for a full element
-    const double* __restrict__ M1;       // [n][P1*P1]
-    const double* __restrict__ Kt1;      // [3][n][P1*P1]
-    const double* __restrict__ TM;       // [nta][D*D]
-    const double* __restrict__ TA;       // [nta][D*D]  a_mass*TM + TK_x
-    const double* __restrict__ TK;       // [3][nta][D*D]
-    const CT* __restrict__ cut_mats;     // [ncut][P*P]
+    const int* item_list;  // >= 0: tile id; < 0: cut chunk -(k+1)
+    const int* tile_kind;
+    const int* tile_eptr;
+    const int* tile_elem;
+    const int* tile_ecut;  // unused by the device (cut elements are separate items)
+    const double* M1;
+    const double* Kt1;
+    const double* TM;
+    const double* TA;
+    const double* TK;
+    const int* cut_base;       // [n_cut] full DOF index of the element's first DOF
+    const int* cut_dof_slot;   // [n_full] slot in the DOF -> cut list, -1 if none
+    const int* cut_dof_ptr;    // [n_slots + 1]
+    const int* cut_dof_ent;    // cut * P + local
     ExtDev ext;
-    double* ypart;                       // [nta^3][D^3]
+    double* ypart;             // [nta^3][D^3]
+    double* ycut;              // [n_cut][P]
+    unsigned* work;            // dynamic work counter (reset in phase 2)
+};
 
-    __device__ __forceinline__ int D3() const { return D * D * D; }
+template <typename CT, int P1>
+struct TileOp {
+    static constexpr int P = P1 * P1 * P1;
+    static constexpr int PP = P1 * P1;
+    static constexpr int T = 4;
+    static constexpr int D = T + P1 - 1;
+    static constexpr int D3 = D * D * D;
+    static constexpr int NW = CUTCELL_WARPS;
+    // shared-memory sub-arrays start on 16-byte boundaries (even double counts)
+    static constexpr int D3a = (D3 + 1) & ~1;
+    static constexpr int Pa = (P + 1) & ~1;
+    static constexpr int CTRL = 2;  // doubles reserved for the work-item slot
+    TileData td;
+    const CT* __restrict__ cut_mats;
 
-    // ---- phase 1: one tile -> ypart ---------------------------------------
-    __device__ void tile_apply(const double* pred, int tile, double* sm) const {
-        typedef typename Conv<CT>::acc acc_t;
-        const int d3 = D3();
-        const int tx = tile % nta, ty = (tile / nta) % nta, tz = tile / (nta * nta);
-        double* xs = sm;               // D^3
-        double* out = ypart + (size_t)tile * d3;
-        for (int k = threadIdx.x; k < d3; k += blockDim.x) {
+    static size_t smem_bytes() {
+        const size_t full = 5 * (size_t)D3a;
+        const size_t mixed = (size_t)D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa + 3 * 4 * 2 * PP;
+        const size_t cut = (size_t)Pa;
+        size_t m = full > mixed ? full : mixed;
+        return (CTRL + (m > cut ? m : cut)) * sizeof(double);
+    }
+
+    __device__ __forceinline__ void gather_window(const double* pred, int tx, int ty, int tz, double* xs) const {
+        const int nb = td.nb;
+        for (int k = threadIdx.x; k < D3; k += blockDim.x) {
             const int dx = k % D, dy = (k / D) % D, dz = k / (D * D);
             const int gx = tx * T + dx, gy = ty * T + dy, gz = tz * T + dz;
             double v = 0.0;
-            if (gx < nb && gy < nb && gz < nb) v = ext.gather(pred, (gz * nb + gy) * nb + gx);
+            if (gx < nb && gy < nb && gz < nb) v = td.ext.gather(pred, (gz * nb + gy) * nb + gx);
             xs[k] = v;
         }
-        __syncthreads();
-        const int kind = __ldg(tile_kind + tile);
-        if (kind == TILE_FULL) {
-            double* u1 = xs + d3;
-            double* u2 = u1 + d3;
-            double* v1 = u2 + d3;
-            double* v2 = v1 + d3;
-            const double* Mx = TM + (size_t)tx * D * D;
-            const double* Ax = TA + (size_t)tx * D * D;
-            const double* My = TM + (size_t)ty * D * D;
-            const double* Ky = TK + ((size_t)1 * nta + ty) * D * D;
-            const double* Mz = TM + (size_t)tz * D * D;
-            const double* Kz = TK + ((size_t)2 * nta + tz) * D * D;
-            // x passes
-            for (int k = threadIdx.x; k < d3; k += blockDim.x) {
-                const int i = k % D, row = k - i;
-                const int j0 = max(0, i - p), j1 = min(D - 1, i + p);
-                double s1 = 0.0, s2 = 0.0;
-                for (int j = j0; j <= j1; ++j) {
+    }
+
+    __device__ void full_tile(int tx, int ty, int tz, double* xs, double* out) const {
+        double* u1 = xs + D3a;
+        double* u2 = u1 + D3a;
+        double* v1 = u2 + D3a;
+        double* v2 = v1 + D3a;
+        const int nta = td.nta;
+        const double* Mx = td.TM + (size_t)tx * D * D;
+        const double* Ax = td.TA + (size_t)tx * D * D;
+        const double* My = td.TM + (size_t)ty * D * D;
+        const double* Ky = td.TK + ((size_t)1 * nta + ty) * D * D;
+        const double* Mz = td.TM + (size_t)tz * D * D;
+        const double* Kz = td.TK + ((size_t)2 * nta + tz) * D * D;
+        constexpr int p = P1 - 1;
+        for (int k = threadIdx.x; k < D3; k += blockDim.x) {
+            const int i = k % D, row = k - i;
+            double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+            for (int o = -p; o <= p; ++o) {
+                const int j = i + o;
+                if (j >= 0 && j < D) {
                     const double xv = xs[row + j];
                     s1 += __ldg(Mx + i * D + j) * xv;
                     s2 += __ldg(Ax + i * D + j) * xv;
                 }
-                u1[k] = s1;
-                u2[k] = s2;
             }
-            __syncthreads();
-            // y passes: v1 = My u1, v2 = My u2 + Ky u1
-            for (int k = threadIdx.x; k < d3; k += blockDim.x) {
-                const int x = k % D, i = (k / D) % D, z = k / (D * D);
-                const int j0 = max(0, i - p), j1 = min(D - 1, i + p);
-                double s1 = 0.0, s2 = 0.0;
-                for (int j = j0; j <= j1; ++j) {
-                    const int o = (z * D + j) * D + x;
-                    const double m = __ldg(My + i * D + j);
-                    s1 += m * u1[o];
-                    s2 += m * u2[o] + __ldg(Ky + i * D + j) * u1[o];
-                }
-                v1[k] = s1;
-                v2[k] = s2;
-            }
-            __syncthreads();
-            // z passes: out = Mz v2 + Kz v1
-            for (int k = threadIdx.x; k < d3; k += blockDim.x) {
-                const int xy = k % (D * D), i = k / (D * D);
-                const int j0 = max(0, i - p), j1 = min(D - 1, i + p);
-                double s = 0.0;
-                for (int j = j0; j <= j1; ++j) {
-                    const int o = j * D * D + xy;
-                    s += __ldg(Mz + i * D + j) * v2[o] + __ldg(Kz + i * D + j) * v1[o];
-                }
-                out[k] = s;
-            }
-            __syncthreads();
-            return;
+            u1[k] = s1;
+            u2[k] = s2;
         }
-        // ---- mixed tile: element by element, one warp per element --------
+        __syncthreads();
+        for (int k = threadIdx.x; k < D3; k += blockDim.x) {
+            const int x = k % D, i = (k / D) % D, z = k / (D * D);
+            double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+            for (int o = -p; o <= p; ++o) {
+                const int j = i + o;
+                if (j >= 0 && j < D) {
+                    const int q = (z * D + j) * D + x;
+                    const double m = __ldg(My + i * D + j);
+                    s1 += m * u1[q];
+                    s2 += m * u2[q] + __ldg(Ky + i * D + j) * u1[q];
+                }
+            }
+            v1[k] = s1;
+            v2[k] = s2;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < D3; k += blockDim.x) {
+            const int xy = k % (D * D), i = k / (D * D);
+            double s = 0.0;
+#pragma unroll
+            for (int o = -p; o <= p; ++o) {
+                const int j = i + o;
+                if (j >= 0 && j < D) {
+                    const int q = j * D * D + xy;
+                    s += __ldg(Mz + i * D + j) * v2[q] + __ldg(Kz + i * D + j) * v1[q];
+                }
+            }
+            out[k] = s;
+        }
+    }
+
+    __device__ void mixed_tile(int tile, int tx, int ty, int tz, double* xs, double* out) const {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        const int nw = blockDim.x >> 5;
-        double* acc = xs + d3 + (size_t)warp * d3;            // per-warp accumulator
-        double* e0 = xs + d3 + (size_t)nw * d3 + (size_t)warp * 4 * P;
-        double* e1 = e0 + P;
-        double* e2 = e1 + P;
-        double* e3 = e2 + P;
-        for (int k = lane; k < d3; k += 32) acc[k] = 0.0;
-        const int eb = __ldg(tile_eptr + tile), ee = __ldg(tile_eptr + tile + 1);
-        const int P1sq = P1 * P1;
-        for (int it = eb + warp; it < ee; it += nw) {
-            const int le = __ldg(tile_elem + it);
+        double* acc = xs + D3a + (size_t)warp * D3a;
+        double* e0 = xs + D3a + (size_t)NW * D3a + (size_t)warp * 4 * Pa;
+        double* e1 = e0 + Pa;
+        double* e2 = e1 + Pa;
+        double* e3 = e2 + Pa;
+        double* fac = xs + D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa;  // [axis][4 pos][M, K~][PP]
+        const int n = td.n;
+        for (int k = threadIdx.x; k < 3 * 4 * 2 * PP; k += blockDim.x) {
+            const int e = k % PP, w = (k / PP) % 2, pos = (k / (2 * PP)) % 4, ax = k / (8 * PP);
+            const int t = ax == 0 ? tx : (ax == 1 ? ty : tz);
+            const int el = min(t * T + pos, n - 1);
+            double v = w == 0 ? __ldg(td.M1 + (size_t)el * PP + e) : __ldg(td.Kt1 + ((size_t)ax * n + el) * PP + e);
+            if (ax == 0 && w == 1) v += td.a_mass * __ldg(td.M1 + (size_t)el * PP + e);  // a M + K~ on x
+            fac[k] = v;
+        }
+        for (int k = lane; k < D3; k += 32) acc[k] = 0.0;
+        __syncthreads();
+        const int eb = __ldg(td.tile_eptr + tile), ee = __ldg(td.tile_eptr + tile + 1);
+        for (int it = eb + warp; it < ee; it += NW) {
+            const int le = __ldg(td.tile_elem + it);
             const int lx = le % T, ly = (le / T) % T, lz = le / (T * T);
-            const int cut = __ldg(tile_ecut + it);
+            const double* Mx = fac + ((0 * 4 + lx) * 2 + 0) * PP;
+            const double* Ax = fac + ((0 * 4 + lx) * 2 + 1) * PP;
+            const double* My = fac + ((1 * 4 + ly) * 2 + 0) * PP;
+            const double* Ky = fac + ((1 * 4 + ly) * 2 + 1) * PP;
+            const double* Mz = fac + ((2 * 4 + lz) * 2 + 0) * PP;
+            const double* Kz = fac + ((2 * 4 + lz) * 2 + 1) * PP;
             __syncwarp();
             for (int k = lane; k < P; k += 32) {
-                const int a = k % P1, b = (k / P1) % P1, c = k / P1sq;
+                const int a = k % P1, b = (k / P1) % P1, c = k / PP;
                 e0[k] = xs[((lz + c) * D + (ly + b)) * D + (lx + a)];
             }
             __syncwarp();
-            if (cut >= 0) {
-                const CT* A = cut_mats + (size_t)cut * P * P;
-                for (int r0 = 0; r0 < P; r0 += 32) {
-                    const int r = r0 + lane;
-                    acc_t s = 0;
-                    if (r < P) {
-                        for (int c = 0; c < P; ++c) s += Conv<CT>::ld(A + (size_t)c * P + r) * (acc_t)e0[c];
-                        const int a = r % P1, b = (r / P1) % P1, cc = r / P1sq;
-                        acc[((lz + cc) * D + (ly + b)) * D + (lx + a)] += (double)s;
-                    }
+            for (int k = lane; k < P; k += 32) {
+                const int i = k % P1, row = k - i;
+                double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int j = 0; j < P1; ++j) {
+                    s1 += Mx[i * P1 + j] * e0[row + j];
+                    s2 += Ax[i * P1 + j] * e0[row + j];
                 }
-            } else {
-                const int ex = tx * T + lx, ey = ty * T + ly, ez = tz * T + lz;
-                const double* Mx = M1 + (size_t)ex * P1sq;
-                const double* Kx = Kt1 + (size_t)ex * P1sq;
-                const double* My = M1 + (size_t)ey * P1sq;
-                const double* Ky = Kt1 + ((size_t)n + ey) * P1sq;
-                const double* Mz = M1 + (size_t)ez * P1sq;
-                const double* Kz = Kt1 + ((size_t)2 * n + ez) * P1sq;
-                for (int k = lane; k < P; k += 32) {
-                    const int i = k % P1, row = k - i;
-                    double s1 = 0.0, s2 = 0.0;
-                    for (int j = 0; j < P1; ++j) {
-                        const double m = __ldg(Mx + i * P1 + j);
-                        s1 += m * e0[row + j];
-                        s2 += (a_mass * m + __ldg(Kx + i * P1 + j)) * e0[row + j];
-                    }
-                    e1[k] = s1;
-                    e2[k] = s2;
+                e1[k] = s1;
+                e2[k] = s2;
+            }
+            __syncwarp();
+            for (int k = lane; k < P; k += 32) {
+                const int x = k % P1, i = (k / P1) % P1, z = k / PP;
+                double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int j = 0; j < P1; ++j) {
+                    const int q = (z * P1 + j) * P1 + x;
+                    s1 += My[i * P1 + j] * e1[q];
+                    s2 += My[i * P1 + j] * e2[q] + Ky[i * P1 + j] * e1[q];
                 }
-                __syncwarp();
-                for (int k = lane; k < P; k += 32) {
-                    const int x = k % P1, i = (k / P1) % P1, z = k / P1sq;
-                    double s1 = 0.0, s2 = 0.0;
-                    for (int j = 0; j < P1; ++j) {
-                        const int o = (z * P1 + j) * P1 + x;
-                        const double m = __ldg(My + i * P1 + j);
-                        s1 += m * e1[o];
-                        s2 += m * e2[o] + __ldg(Ky + i * P1 + j) * e1[o];
-                    }
-                    e3[k] = s1;
-                    e0[k] = s2;  // e0 no longer needed as input
+                e3[k] = s1;
+                e0[k] = s2;
+            }
+            __syncwarp();
+            for (int k = lane; k < P; k += 32) {
+                const int xy = k % PP, i = k / PP;
+                double s = 0.0;
+#pragma unroll
+                for (int j = 0; j < P1; ++j) {
+                    const int q = j * PP + xy;
+                    s += Mz[i * P1 + j] * e0[q] + Kz[i * P1 + j] * e3[q];
                 }
-                __syncwarp();
-                for (int k = lane; k < P; k += 32) {
-                    const int xy = k % P1sq, i = k / P1sq;
-                    double s = 0.0;
-                    for (int j = 0; j < P1; ++j) {
-                        const int o = j * P1sq + xy;
-                        s += __ldg(Mz + i * P1 + j) * e0[o] + __ldg(Kz + i * P1 + j) * e3[o];
-                    }
-                    const int a = xy % P1, b = xy / P1;
-                    acc[((lz + i) * D + (ly + b)) * D + (lx + a)] += s;
-                }
+                acc[((lz + i) * D + (ly + xy / P1)) * D + (lx + xy % P1)] += s;
             }
         }
         __syncthreads();
-        double* acc0 = xs + d3;
-        for (int k = threadIdx.x; k < d3; k += blockDim.x) {
+        double* acc0 = xs + D3a;
+        for (int k = threadIdx.x; k < D3; k += blockDim.x) {
             double s = 0.0;
-            for (int w = 0; w < nw; ++w) s += acc0[(size_t)w * d3 + k];
+#pragma unroll
+            for (int w = 0; w < NW; ++w) s += acc0[(size_t)w * D3a + k];
             out[k] = s;
+        }
+    }
+
+    // one cut element: x_e gathered through E, y_e = A_e x_e -> ycut[c]
+    __device__ void cut_element(const double* pred, int c, double* xe) const {
+        typedef typename Conv<CT>::acc acc_t;
+        const int nb = td.nb;
+        const int base = __ldg(td.cut_base + c);
+        for (int k = threadIdx.x; k < P; k += blockDim.x) {
+            const int a = k % P1, b = (k / P1) % P1, cc = k / PP;
+            xe[k] = td.ext.gather(pred, base + (cc * nb + b) * nb + a);
+        }
+        __syncthreads();
+        const CT* A = cut_mats + (size_t)c * P * P;
+        const int q = threadIdx.x & 3;
+        if (!CUTCELL_OK_IF(CUTCELL_ALIGNED(A, sizeof(CT)) && c < td.n_cut, 11, c, td.work + 1)) {
+            __syncthreads();
+            return;
+        }
+        for (int r0 = 0; r0 < P; r0 += (int)(blockDim.x >> 2)) {
+            const int r = r0 + (int)(threadIdx.x >> 2);
+            acc_t s = 0;
+            if (r < P) {
+                const CT* Ar = A + (size_t)r * P;
+#pragma unroll 8
+                for (int col = q; col < P; col += 4) s += Conv<CT>::ld(Ar + col) * (acc_t)xe[col];
+            }
+            s += __shfl_xor_sync(0xffffffffu, s, 1);
+            s += __shfl_xor_sync(0xffffffffu, s, 2);
+            if (r < P && q == 0 && CUTCELL_OK_IF(CUTCELL_ALIGNED(td.ycut + (size_t)c * P + r, 8), 12, r, td.work + 1))
+                td.ycut[(size_t)c * P + r] = (double)s;
         }
         __syncthreads();
     }
 
-    // ---- phase 2 helpers ---------------------------------------------------
+    __device__ void phase1(const double* pred, double* smem) const {
+        int& s_item = *reinterpret_cast<int*>(smem);
+        double* sm = smem + CTRL;
+#ifdef CUTCELL_DEBUG_CHECKS
+        unsigned* dbgw = td.work + 1;
+        if (threadIdx.x == 0) {
+            CUTCELL_OK_IF(CUTCELL_ALIGNED(sm, 16), 1, 0, dbgw);
+            CUTCELL_OK_IF(CUTCELL_ALIGNED(cut_mats, sizeof(CT)), 2, 0, dbgw);
+            CUTCELL_OK_IF(CUTCELL_ALIGNED(td.ypart, 8) && CUTCELL_ALIGNED(td.ycut, 8), 3, 0, dbgw);
+            CUTCELL_OK_IF(CUTCELL_ALIGNED(td.M1, 8) && CUTCELL_ALIGNED(td.Kt1, 8) && CUTCELL_ALIGNED(td.TM, 8) &&
+                              CUTCELL_ALIGNED(td.TA, 8) && CUTCELL_ALIGNED(td.TK, 8),
+                          4, 0, dbgw);
+            CUTCELL_OK_IF(CUTCELL_ALIGNED(pred, 8), 5, 0, dbgw);
+            CUTCELL_OK_IF(CUTCELL_ALIGNED(td.ext.small_val, 8) && CUTCELL_ALIGNED(td.ext.smallT_val, 8), 6, 0, dbgw);
+            CUTCELL_OK_IF(CUTCELL_ALIGNED(&s_item, 4), 7, 0, dbgw);
+        }
+#else
+        unsigned* dbgw = nullptr;
+#endif
+        (void)dbgw;
+        while (true) {
+            if (threadIdx.x == 0) s_item = (int)atomicAdd(td.work, 1u);
+            __syncthreads();
+            const int item = s_item;
+            __syncthreads();
+            if (item >= td.n_items) break;
+            if (!CUTCELL_OK_IF(item >= 0, 8, item, td.work + 1)) break;
+            const int code = __ldg(td.item_list + item);
+            if (code >= 0) {
+                const int tile = code;
+                const int nta = td.nta;
+                if (!CUTCELL_OK_IF(tile < nta * nta * nta, 9, tile, td.work + 1)) continue;
+                const int tx = tile % nta, ty = (tile / nta) % nta, tz = tile / (nta * nta);
+                double* xs = sm;
+                gather_window(pred, tx, ty, tz, xs);
+                __syncthreads();
+                double* out = td.ypart + (size_t)tile * D3;
+                if (__ldg(td.tile_kind + tile) == TILE_FULL)
+                    full_tile(tx, ty, tz, xs, out);
+                else
+                    mixed_tile(tile, tx, ty, tz, xs, out);
+                __syncthreads();
+            } else {
+                const int c0 = (-code - 1) * td.cut_chunk;
+                const int c1 = min(c0 + td.cut_chunk, td.n_cut);
+                if (!CUTCELL_OK_IF(c0 >= 0 && c0 < td.n_cut, 10, c0, td.work + 1)) continue;
+                for (int c = c0; c < c1; ++c) cut_element(pred, c, sm);
+            }
+        }
+    }
+
     __device__ __forceinline__ double yfull(int i) const {
+        const int nb = td.nb, nta = td.nta;
         const int ix = i % nb, iy = (i / nb) % nb, iz = i / (nb * nb);
-        int t1x = min(ix / T, nta - 1), t1y = min(iy / T, nta - 1), t1z = min(iz / T, nta - 1);
-        const int d3 = D3();
+        const int t1x = min(ix / T, nta - 1), t1y = min(iy / T, nta - 1), t1z = min(iz / T, nta - 1);
         double s = 0.0;
         for (int tz = t1z - 1; tz <= t1z; ++tz) {
             if (tz < 0 || iz - tz * T >= D) continue;
@@ -290,37 +405,39 @@ struct TileOp {
                 for (int tx = t1x - 1; tx <= t1x; ++tx) {
                     if (tx < 0 || ix - tx * T >= D) continue;
                     const int tile = (tz * nta + ty) * nta + tx;
-                    s += __ldcg(ypart + (size_t)tile * d3 + ((iz - tz * T) * D + (iy - ty * T)) * D + (ix - tx * T));
+                    s += __ldcg(td.ypart + (size_t)tile * D3 + ((iz - tz * T) * D + (iy - ty * T)) * D + (ix - tx * T));
                 }
+            }
+        }
+        const int slot = __ldg(td.cut_dof_slot + i);
+        if (slot >= 0) {
+            const int k1 = __ldg(td.cut_dof_ptr + slot + 1);
+            for (int k = __ldg(td.cut_dof_ptr + slot); k < k1; ++k) {
+                const int e = __ldg(td.cut_dof_ent + k);
+                if (CUTCELL_OK_IF(e >= 0 && e < td.n_cut * P, 13, e, td.work + 1)) s += __ldcg(td.ycut + e);
             }
         }
         return s;
     }
 
     __device__ __forceinline__ double scatter_row(int j) const {
-        double y = yfull(__ldg(ext.full_of_red + j));
-        const int k1 = __ldg(ext.smallT_ptr + j + 1);
-        for (int k = __ldg(ext.smallT_ptr + j); k < k1; ++k)
-            y += __ldg(ext.smallT_val + k) * yfull(__ldg(ext.smallT_row + k));
+        double y = yfull(__ldg(td.ext.full_of_red + j));
+        const int k1 = __ldg(td.ext.smallT_ptr + j + 1);
+        for (int k = __ldg(td.ext.smallT_ptr + j); k < k1; ++k)
+            y += __ldg(td.ext.smallT_val + k) * yfull(__ldg(td.ext.smallT_row + k));
         return y;
     }
 
     __device__ __forceinline__ double apply(const double* p, double* y, const GridSync& gs, double* sm) const {
-        for (int li = blockIdx.x; li < ntile_list; li += gridDim.x) tile_apply(p, __ldg(tile_list + li), sm);
+        phase1(p, sm);
         if (!grid_sync(gs)) return 0.0;
+        if (blockIdx.x == 0 && threadIdx.x == 0) *td.work = 0u;  // every block has left phase 1
         double part = 0.0;
-        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < ext.n_red; j += gridDim.x * blockDim.x) {
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < td.ext.n_red; j += gridDim.x * blockDim.x) {
             const double yj = scatter_row(j);
             y[j] = yj;
             part += __ldcg(p + j) * yj;
         }
         return part;
-    }
-
-    static size_t smem_bytes(int D, int P, int nwarps) {
-        const size_t d3 = (size_t)D * D * D;
-        size_t full = 5 * d3;
-        size_t mixed = d3 + (size_t)nwarps * d3 + (size_t)nwarps * 4 * P;
-        return (full > mixed ? full : mixed) * sizeof(double);
     }
 };

@@ -38,7 +38,7 @@ struct PcgBufs {
 // iteration count and *rel the final recursive relative residual.
 template <class Op>
 __device__ int pcg_core(const Op& op, const PcgBufs& B, const double* rhs, double* d, double tol, int maxiter,
-                        const GridSync& gs, double* sm, double* sh, double rhs_norm_override, int* iters,
+                        const GridSync& gs, double* sm, double* sh, double diverge, int* iters,
                         double* rel_out) {
     const int n = B.n;
     const int nb = gridDim.x;
@@ -64,7 +64,6 @@ __device__ int pcg_core(const Op& op, const PcgBufs& B, const double* rhs, doubl
     if (!grid_sync(gs)) return CUTCELL_E_BARRIER;
     double rz = grid_reduce(part + 0 * nb, nb, sh);
     double bnorm = sqrt(grid_reduce(part + 1 * nb, nb, sh));
-    if (rhs_norm_override > 0.0) bnorm = rhs_norm_override;
     if (bnorm == 0.0) bnorm = 1.0;
     int status = CUTCELL_E_NOCONV;
     int k = 0;
@@ -106,6 +105,10 @@ __device__ int pcg_core(const Op& op, const PcgBufs& B, const double* rhs, doubl
         }
         if (rel <= tol) {
             status = CUTCELL_OK;
+            break;
+        }
+        if (diverge > 0.0 && rel > diverge) {  // inner solve of a refinement sweep ran away
+            status = CUTCELL_E_NAN;
             break;
         }
         const double beta = rzn / rz;
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) pcg_kernel(Op op, SolveArgs 
     __shared__ double sh[CUTCELL_WARPS + 1];
     int iters = 0;
     double rel = 1.0;
-    int status = pcg_core(op, a.B, a.b, a.x, a.tol, a.maxiter, a.gs, sm, sh, -1.0, &iters, &rel);
+    int status = pcg_core(op, a.B, a.b, a.x, a.tol, a.maxiter, a.gs, sm, sh, 0.0, &iters, &rel);
     double true_rel = -1.0;
     if (status != CUTCELL_E_BARRIER && !grid_error(a.gs)) {
         const double bn = norm_of(a.b, a.B.n, a.B.part, a.gs, sh, 6);
@@ -198,6 +201,20 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) ir_kernel(OpHi hi, OpLo lo, 
     const int n = a.B.n;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
+#ifdef CUTCELL_DEBUG_CHECKS
+    if (threadIdx.x == 0) {
+        unsigned* w = a.gs.count + 4;
+        CUTCELL_OK_IF(CUTCELL_ALIGNED(a.x, 8) && CUTCELL_ALIGNED(a.b, 8) && CUTCELL_ALIGNED(a.d, 8) &&
+                          CUTCELL_ALIGNED(a.rhat, 8),
+                      20, 0, w);
+        CUTCELL_OK_IF(CUTCELL_ALIGNED(a.B.r, 8) && CUTCELL_ALIGNED(a.B.p, 8) && CUTCELL_ALIGNED(a.B.Ap, 8) &&
+                          CUTCELL_ALIGNED(a.B.dinv, 8) && CUTCELL_ALIGNED(a.B.part, 8),
+                      21, 0, w);
+        CUTCELL_OK_IF(CUTCELL_ALIGNED(a.res, 8) && CUTCELL_ALIGNED(a.gs.count, 4) && CUTCELL_ALIGNED(a.gs.err, 4), 22, 0,
+                      w);
+        CUTCELL_OK_IF(CUTCELL_ALIGNED(sm, 16) && CUTCELL_ALIGNED(sh, 8), 23, 0, w);
+    }
+#endif
     for (int i = gtid; i < n; i += gstride) {
         a.x[i] = 0.0;
         a.rhat[i] = a.b[i];
@@ -206,16 +223,23 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) ir_kernel(OpHi hi, OpLo lo, 
     if (bn == 0.0) bn = 1.0;
     int total = 0, outer = 0;
     int status = CUTCELL_E_NOCONV;
-    double true_rel = 1.0, rel_in = 1.0;
+    double true_rel = 1.0, rel_in = 1.0, prev = 1.0;
+    int stall = 0;
     for (outer = 1; outer <= a.max_outer; ++outer) {
         int it = 0;
         const int budget = a.maxiter - total;
         if (budget <= 0) break;
+        // the inner solve may not grow its residual by more than 1e3: a
+        // reduced-precision operator that lost definiteness stops the sweep
         int st = pcg_core(lo, a.B, a.rhat, a.d, a.inner_tol, budget < a.inner_maxiter ? budget : a.inner_maxiter,
-                          a.gs, sm, sh, -1.0, &it, &rel_in);
+                          a.gs, sm, sh, 1.0e3, &it, &rel_in);
         total += it;
         if (st == CUTCELL_E_BARRIER) {
             status = st;
+            break;
+        }
+        if (st == CUTCELL_E_NAN || (st == CUTCELL_E_BREAKDOWN && it <= 1)) {
+            status = CUTCELL_E_BREAKDOWN;  // correction discarded, x keeps the last refined iterate
             break;
         }
         for (int i = gtid; i < n; i += gstride) a.x[i] += a.d[i];
@@ -236,8 +260,11 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) ir_kernel(OpHi hi, OpLo lo, 
             status = CUTCELL_OK;
             break;
         }
-        if (st == CUTCELL_E_BREAKDOWN && it <= 1) {
-            status = st;
+        // stagnation: two sweeps in a row that do not halve the true residual
+        stall = (true_rel > 0.5 * prev) ? stall + 1 : 0;
+        prev = true_rel;
+        if (stall >= 2) {
+            status = CUTCELL_E_NOCONV;
             break;
         }
     }

@@ -58,13 +58,14 @@ class CutcellTileDesc(C.Structure):
         ("degree", C.c_int32),
         ("tile", C.c_int32),
         ("n_tiles_axis", C.c_int32),
-        ("n_tile_list", C.c_int32),
+        ("n_items", C.c_int32),
+        ("cut_chunk", C.c_int32),
         ("n_cut", C.c_int32),
         ("n_full", C.c_int32),
         ("n_red", C.c_int32),
         ("n_small", C.c_int32),
         ("a_mass", C.c_double),
-        ("tile_list", _P),
+        ("item_list", _P),
         ("tile_kind", _P),
         ("tile_eptr", _P),
         ("tile_elem", _P),
@@ -75,6 +76,10 @@ class CutcellTileDesc(C.Structure):
         ("TA", _P),
         ("TK", _P),
         ("cut_mats", _P),
+        ("cut_base", _P),
+        ("cut_dof_slot", _P),
+        ("cut_dof_ptr", _P),
+        ("cut_dof_ent", _P),
         ("red_of_full", _P),
         ("small_slot", _P),
         ("small_ptr", _P),

@@ -28,7 +28,22 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def build_setup(force: bool = False) -> Path:
+    """Host setup library (g++ -O3 -fopenmp), no CUDA."""
+    out = PKG / "libcutcell_setup.so"
+    src = CSRC / "cutcell_setup.cpp"
+    hdr = ROOT.parent / "include" / "cutcell_setup.h"
+    if out.exists() and not force and all(out.stat().st_mtime >= d.stat().st_mtime for d in (src, hdr)):
+        return out
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-std=c++17", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", str(src), "-o", str(out) + ".tmp"]
+    subprocess.run(cmd, check=True, cwd=str(ROOT))
+    os.replace(str(out) + ".tmp", out)
+    return out
+
+
 def build(verbose: bool = False, force: bool = False) -> Path:
+    build_setup(force=force)
     out = PKG / "libcutcell_b200.so"
     deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + [ROOT.parent / "include" / "cutcell_b200.h"]
     if out.exists() and not force and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps if d.exists()):

@@ -35,26 +35,34 @@ class TileLayout:
     tile: int
     n_tiles_axis: int
     tile_kind: np.ndarray  # (nta^3,) int32
-    tile_list: np.ndarray  # nonempty tiles in work order
-    tile_eptr: np.ndarray  # (nta^3 + 1,)
+    item_list: np.ndarray  # work items, >= 0 tile id, < 0 cut chunk -(k+1)
+    tile_eptr: np.ndarray  # (nta^3 + 1,) uncut elements of mixed tiles
     tile_elem: np.ndarray
-    tile_ecut: np.ndarray
     TM: np.ndarray  # (nta, D, D)
     TA: np.ndarray
     TK: np.ndarray  # (3, nta, D, D)
+    cut_chunk: int
+    cut_base: np.ndarray  # (ncut,) first full DOF of each cut element
+    cut_dof_slot: np.ndarray  # (n_full,)
+    cut_dof_ptr: np.ndarray
+    cut_dof_ent: np.ndarray  # cut * P + local row
+
+    @property
+    def tile_list(self) -> np.ndarray:
+        return self.item_list[self.item_list >= 0]
 
 
-def build_tile_layout(prob: CutCellProblem, tile: int = 4) -> TileLayout:
+def build_tile_layout(prob: CutCellProblem, tile: int = 4, cut_chunk: int = 2) -> TileLayout:
     n, p = prob.n_elements, prob.degree
     T = int(tile)
     nta = -(-n // T)
     D = T + p
+    nb = n + p
+    P = prob.P
     et = prob.elem_type
-    cut_index = np.full(n * n * n, -1, dtype=np.int64)
-    cut_index[prob.cut_ids] = np.arange(prob.cut_ids.size)
     kind = np.zeros(nta**3, dtype=np.int32)
     eptr = np.zeros(nta**3 + 1, dtype=np.int32)
-    elems, ecuts = [], []
+    elems = []
     mixed_cost = {}
     for tz in range(nta):
         for ty in range(nta):
@@ -64,21 +72,19 @@ def build_tile_layout(prob: CutCellProblem, tile: int = 4) -> TileLayout:
                 complete = sub.shape == (T, T, T)
                 if complete and np.all(sub == FULL):
                     kind[t] = TILE_FULL
-                elif np.any(sub != 0):
+                elif np.any(sub == FULL):
                     kind[t] = TILE_MIXED
-                    lz, ly, lx = np.nonzero(sub != 0)
-                    loc = (lz * T + ly) * T + lx
-                    glob = ((tz * T + lz) * n + (ty * T + ly)) * n + (tx * T + lx)
-                    elems.append(loc.astype(np.int32))
-                    ecuts.append(cut_index[glob].astype(np.int32))
-                    mixed_cost[t] = int(loc.size + 4 * np.count_nonzero(cut_index[glob] >= 0))
+                    lz, ly, lx = np.nonzero(sub == FULL)
+                    elems.append(((lz * T + ly) * T + lx).astype(np.int32))
+                    mixed_cost[t] = int(lx.size)
                 eptr[t + 1] = eptr[t] + (elems[-1].size if kind[t] == TILE_MIXED else 0)
     tile_elem = np.concatenate(elems) if elems else np.zeros(0, np.int32)
-    tile_ecut = np.concatenate(ecuts) if ecuts else np.zeros(0, np.int32)
-    # work order: heaviest mixed tiles first, then full tiles
-    mixed = sorted(mixed_cost, key=lambda t: -mixed_cost[t])
+    ncut = int(prob.cut_ids.size)
+    nchunk = -(-ncut // cut_chunk)
+    # work order: heaviest mixed tiles, cut chunks, then full tiles
+    mixed = sorted(mixed_cost, key=lambda t: (-mixed_cost[t], t))
     full = [int(t) for t in np.nonzero(kind == TILE_FULL)[0]]
-    tile_list = np.array(mixed + full, dtype=np.int32)
+    item_list = np.array(mixed + [-(k + 1) for k in range(nchunk)] + full, dtype=np.int32)
     # tile-assembled 1D factors
     TM = np.zeros((nta, D, D))
     TK = np.zeros((3, nta, D, D))
@@ -92,7 +98,24 @@ def build_tile_layout(prob: CutCellProblem, tile: int = 4) -> TileLayout:
             for ax in range(3):
                 TK[ax, t, sl, sl] += prob.Kt1[ax, e]
     TA = prob.a_mass * TM + TK[0]
-    return TileLayout(T, nta, kind, tile_list, eptr, tile_elem, tile_ecut, TM, TA, TK)
+    # cut elements: first DOF and the DOF -> (cut, local row) lists
+    cz, cy, cx = np.unravel_index(prob.cut_ids, (n, n, n))
+    cut_base = ((cz * nb + cy) * nb + cx).astype(np.int32)
+    slot = np.full(prob.n_full, -1, dtype=np.int32)
+    if ncut:
+        R = prob.element_rows(cx, cy, cz)  # (ncut, P)
+        g = R.ravel()
+        ent = (np.arange(ncut)[:, None] * P + np.arange(P)[None, :]).ravel()
+        order = np.lexsort((ent, g))
+        g, ent = g[order], ent[order]
+        uniq, start = np.unique(g, return_index=True)
+        slot[uniq] = np.arange(uniq.size, dtype=np.int32)
+        ptr = np.append(start, g.size).astype(np.int32)
+        ent = ent.astype(np.int32)
+    else:
+        ptr = np.zeros(1, dtype=np.int32)
+        ent = np.zeros(0, dtype=np.int32)
+    return TileLayout(T, nta, kind, item_list, eptr, tile_elem, TM, TA, TK, cut_chunk, cut_base, slot, ptr, ent)
 
 
 def jacobi_diagonal(prob: CutCellProblem, ext: Extension) -> np.ndarray:
@@ -179,11 +202,15 @@ class CutCellOperator:
         dv = self.device
         P = prob.P
         t = {}
-        t["tile_list"] = _dev(lay.tile_list, i32, dv)
+        t["item_list"] = _dev(lay.item_list, i32, dv)
         t["tile_kind"] = _dev(lay.tile_kind, i32, dv)
         t["tile_eptr"] = _dev(lay.tile_eptr, i32, dv)
         t["tile_elem"] = _dev(np.append(lay.tile_elem, 0), i32, dv)
-        t["tile_ecut"] = _dev(np.append(lay.tile_ecut, 0), i32, dv)
+        t["tile_ecut"] = t["tile_elem"]
+        t["cut_base"] = _dev(np.append(lay.cut_base, 0), i32, dv)
+        t["cut_dof_slot"] = _dev(lay.cut_dof_slot, i32, dv)
+        t["cut_dof_ptr"] = _dev(lay.cut_dof_ptr, i32, dv)
+        t["cut_dof_ent"] = _dev(np.append(lay.cut_dof_ent, 0), i32, dv)
         t["M1"] = _dev(prob.M1, f64, dv)
         t["Kt1"] = _dev(prob.Kt1, f64, dv)
         t["TM"] = _dev(lay.TM, f64, dv)
@@ -203,7 +230,8 @@ class CutCellOperator:
         desc.degree = prob.degree
         desc.tile = lay.tile
         desc.n_tiles_axis = lay.n_tiles_axis
-        desc.n_tile_list = int(lay.tile_list.size)
+        desc.n_items = int(lay.item_list.size)
+        desc.cut_chunk = int(lay.cut_chunk)
         desc.n_cut = int(prob.cut_ids.size)
         desc.n_full = prob.n_full
         desc.n_red = ext.n_red

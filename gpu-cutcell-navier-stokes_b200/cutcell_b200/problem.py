@@ -166,10 +166,15 @@ def build_problem(
     quad_order: int | None = None,
     subdiv: int = 1,
     keep_green: bool = False,
+    load_order: int | None = None,
+    native: bool | None = None,
 ) -> CutCellProblem:
     """Assemble the element-structured operator and load for ``{phi > 0}``.
 
-    ``beta = beta_factor (p+1)^2 / h`` as in code/cut_3d_sbp.py:426.  When
+    ``beta = beta_factor (p+1)^2 / h`` as in code/cut_3d_sbp.py:426.  Cut
+    blocks use the order-``quad_order`` rules (default 3p+1: exact for the
+    degree-6p mass integrand); loads use order ``load_order`` (default p+4).
+    ``native`` selects libcutcell_setup.so (default: when it is built).  When
     ``nitsche`` is false only ``a_mass H + a_stiff K`` is assembled (the
     screened-Poisson proxy of benchmarks/gpu_pcg_benchmark_3d.py:49-57).
     """
@@ -286,47 +291,64 @@ def build_problem(
     # --- cut elements ----------------------------------------------------
     cut_lin = np.nonzero(etype.ravel() == CUT)[0]
     P = p1**3
-    cut_mats = np.zeros((cut_lin.size, P, P))
     fracs = np.zeros(n * n * n)
     fracs[full_mask] = 1.0
-    green = {"Q": [np.zeros((cut_lin.size, P, P)) for _ in range(3)], "S": [np.zeros((cut_lin.size, P, P)) for _ in range(3)]} if keep_green else None
-    keep = np.ones(cut_lin.size, dtype=bool)
-    for k, lin in enumerate(cut_lin):
-        ez, ey, ex = np.unravel_index(lin, (n, n, n))
-        lo = np.array([ex, ey, ez], dtype=float) * h
-        cq = cut_cell_quadrature(phi, lo, h, q, subdiv=subdiv, box_faces=nitsche or keep_green)
-        fracs[lin] = cq.volume / h**3
-        if cq.wv.size == 0:
-            keep[k] = False
-            continue
-        phi_v, grad_v = _tensor_local(basis, ex, ey, ez, cq.xv)
-        Wv = cq.wv
-        Mloc = (phi_v * Wv[:, None]).T @ phi_v
-        Kloc = sum((grad_v[d] * Wv[:, None]).T @ grad_v[d] for d in range(3))
-        A = a_mass * Mloc + a_stiff * Kloc
-        if cq.ws.size and (nitsche or keep_green):
-            phi_s, grad_s = _tensor_local(basis, ex, ey, ez, cq.xs)
-            Ws = cq.ws
-            if nitsche:
-                dn = sum(grad_s[d] * cq.ns[:, d : d + 1] for d in range(3))
-                Nloc = (phi_s * Ws[:, None]).T @ dn
-                Mb = (phi_s * Ws[:, None]).T @ phi_s
-                A = A - Nloc - Nloc.T + beta * Mb
+    ql = load_order or (p + 4)
+    use_native = (native is None and not keep_green and _setup_lib() is not None) or native is True
+    green = None
+    if use_native:
+        cut_mats, mdiag, vols, cload, keep = _cut_blocks_native(
+            fc, subdiv, n, p, q, ql, cut_lin, basis, a_mass, a_stiff, nitsche, beta, forcing, dirichlet
+        )
+        fracs[cut_lin] = vols / h**3
+        rows = rows_all[cut_lin]
+        np.add.at(h_cut, rows.ravel(), mdiag.ravel())
+        np.add.at(load, rows.ravel(), cload.ravel())
+    else:
+        cut_mats = np.zeros((cut_lin.size, P, P))
+        green = {"Q": [np.zeros((cut_lin.size, P, P)) for _ in range(3)], "S": [np.zeros((cut_lin.size, P, P)) for _ in range(3)]} if keep_green else None
+        keep = np.ones(cut_lin.size, dtype=bool)
+        for k, lin in enumerate(cut_lin):
+            ez, ey, ex = np.unravel_index(lin, (n, n, n))
+            lo = np.array([ex, ey, ez], dtype=float) * h
+            cq = cut_cell_quadrature(phi, lo, h, q, subdiv=subdiv, box_faces=nitsche or keep_green)
+            fracs[lin] = cq.volume / h**3
+            if cq.wv.size == 0:
+                keep[k] = False
+                continue
+            phi_v, grad_v = _tensor_local(basis, ex, ey, ez, cq.xv)
+            Wv = cq.wv
+            Mloc = (phi_v * Wv[:, None]).T @ phi_v
+            Kloc = sum((grad_v[d] * Wv[:, None]).T @ grad_v[d] for d in range(3))
+            A = a_mass * Mloc + a_stiff * Kloc
+            if cq.ws.size and (nitsche or keep_green):
+                phi_s, grad_s = _tensor_local(basis, ex, ey, ez, cq.xs)
+                Ws = cq.ws
+                if nitsche:
+                    dn = sum(grad_s[d] * cq.ns[:, d : d + 1] for d in range(3))
+                    Nloc = (phi_s * Ws[:, None]).T @ dn
+                    Mb = (phi_s * Ws[:, None]).T @ phi_s
+                    A = A - Nloc - Nloc.T + beta * Mb
+                if keep_green:
+                    for d in range(3):
+                        green["S"][d][k] = (phi_s * (Ws * cq.ns[:, d])[:, None]).T @ phi_s
             if keep_green:
                 for d in range(3):
-                    green["S"][d][k] = (phi_s * (Ws * cq.ns[:, d])[:, None]).T @ phi_s
-        if keep_green:
-            for d in range(3):
-                green["Q"][d][k] = (phi_v * Wv[:, None]).T @ grad_v[d]
-        cut_mats[k] = 0.5 * (A + A.T)
-        rows = rows_all[lin]
-        np.add.at(h_cut, rows, np.diag(Mloc))
-        if forcing is not None:
-            fv = forcing(cq.xv[:, 0], cq.xv[:, 1], cq.xv[:, 2])
-            np.add.at(load, rows, phi_v.T @ (Wv * fv))
-        if nitsche and dirichlet is not None and cq.ws.size:
-            gv = dirichlet(cq.xs[:, 0], cq.xs[:, 1], cq.xs[:, 2])
-            np.add.at(load, rows, (beta * phi_s - dn).T @ (cq.ws * gv))
+                    green["Q"][d][k] = (phi_v * Wv[:, None]).T @ grad_v[d]
+            cut_mats[k] = 0.5 * (A + A.T)
+            rows = rows_all[lin]
+            np.add.at(h_cut, rows, np.diag(Mloc))
+            if forcing is not None or (nitsche and dirichlet is not None):
+                cl = cut_cell_quadrature(phi, lo, h, ql, subdiv=subdiv, box_faces=nitsche)
+                if forcing is not None and cl.wv.size:
+                    pv, _ = _tensor_local(basis, ex, ey, ez, cl.xv)
+                    fv = forcing(cl.xv[:, 0], cl.xv[:, 1], cl.xv[:, 2])
+                    np.add.at(load, rows, pv.T @ (cl.wv * fv))
+                if nitsche and dirichlet is not None and cl.ws.size:
+                    ps, gs = _tensor_local(basis, ex, ey, ez, cl.xs)
+                    dnl = sum(gs[d] * cl.ns[:, d : d + 1] for d in range(3))
+                    gv = dirichlet(cl.xs[:, 0], cl.xs[:, 1], cl.xs[:, 2])
+                    np.add.at(load, rows, (beta * ps - dnl).T @ (cl.ws * gv))
     if not keep.all():
         # zero-volume cells carry nothing; treat them as solid
         for lin in cut_lin[~keep]:
@@ -386,3 +408,99 @@ def _tensor_local(basis: OpenUniformBasis, ex: int, ey: int, ez: int, X: np.ndar
     Nz, Dz = local_values(basis, np.full(m, ez), X[:, 2])
     t = lambda a, b, c: (a[:, :, None, None] * b[:, None, :, None] * c[:, None, None, :]).reshape(m, p1**3)
     return t(Nz, Ny, Nx), [t(Nz, Ny, Dx), t(Nz, Dy, Nx), t(Dz, Ny, Nx)]
+
+
+_SETUP = None
+
+
+def _setup_lib():
+    """libcutcell_setup.so (native host setup), or None when it is not built."""
+    global _SETUP
+    if _SETUP is None:
+        import ctypes as C
+        from pathlib import Path
+
+        path = Path(__file__).resolve().parent / "libcutcell_setup.so"
+        if not path.exists():
+            _SETUP = False
+            return None
+        lib = C.CDLL(str(path))
+        P = C.c_void_p
+        lib.cutcell_setup_count.argtypes = [P, P, P]
+        lib.cutcell_setup_load_points.argtypes = [P, P, P, P, P]
+        lib.cutcell_setup_blocks.argtypes = [P, P, P, P, P, P, P, P, P]
+        lib.cutcell_setup_threads.argtypes = [C.c_int]
+        for f in (lib.cutcell_setup_count, lib.cutcell_setup_load_points, lib.cutcell_setup_blocks, lib.cutcell_setup_threads):
+            f.restype = C.c_int
+        _SETUP = lib
+    return _SETUP or None
+
+
+def _cut_blocks_native(fc, subdiv, n, p, q, ql, cut_lin, basis, a_mass, a_stiff, nitsche, beta, forcing, dirichlet):
+    import ctypes as C
+
+    from .cutgeom import tet_rule, tri_rule
+
+    lib = _setup_lib()
+    s1 = subdiv + 1
+    ez, ey, ex = np.unravel_index(cut_lin, (n, n, n))
+    cells = np.ascontiguousarray(np.stack([ex, ey, ez], axis=1).astype(np.int32))
+    corner = np.empty((cut_lin.size, s1, s1, s1))
+    for dz in range(s1):
+        for dy in range(s1):
+            for dx in range(s1):
+                corner[:, dz, dy, dx] = fc[ez * subdiv + dz, ey * subdiv + dy, ex * subdiv + dx]
+    corner = np.ascontiguousarray(corner.reshape(cut_lin.size, -1))
+    knots = np.ascontiguousarray(basis.knots)
+
+    def rule4(q_):
+        x, w = tet_rule(q_)
+        return np.ascontiguousarray(np.column_stack([x, w]))
+
+    def rule3(q_):
+        x, w = tri_rule(q_)
+        return np.ascontiguousarray(np.column_stack([x, w]))
+
+    tr, sr, trl, srl = rule4(q), rule3(q), rule4(ql), rule3(ql)
+
+    class Desc(C.Structure):
+        _fields_ = [(k, C.c_int32) for k in ("n_elements", "degree", "subdiv", "box_faces", "n_cells", "n_tet", "n_tri", "n_tet_load", "n_tri_load", "pad")] + [
+            (k, C.c_void_p) for k in ("cells", "corner_phi", "knots", "tet_rule", "tri_rule", "tet_load", "tri_load")
+        ] + [(k, C.c_double) for k in ("a_mass", "a_stiff", "nitsche", "beta")]
+
+    d = Desc()
+    d.n_elements, d.degree, d.subdiv, d.box_faces, d.n_cells = n, p, subdiv, int(bool(nitsche)), cut_lin.size
+    d.n_tet, d.n_tri, d.n_tet_load, d.n_tri_load = tr.shape[0], sr.shape[0], trl.shape[0], srl.shape[0]
+    d.cells, d.corner_phi, d.knots = cells.ctypes.data, corner.ctypes.data, knots.ctypes.data
+    d.tet_rule, d.tri_rule, d.tet_load, d.tri_load = tr.ctypes.data, sr.ctypes.data, trl.ctypes.data, srl.ctypes.data
+    d.a_mass, d.a_stiff, d.nitsche, d.beta = float(a_mass), float(a_stiff), 1.0 if nitsche else 0.0, float(beta)
+    nc = cut_lin.size
+    nv = np.zeros(nc, dtype=np.int64)
+    ns = np.zeros(nc, dtype=np.int64)
+    if lib.cutcell_setup_count(C.byref(d), nv.ctypes.data, ns.ctypes.data):
+        raise RuntimeError("cutcell_setup_count failed")
+    voff = np.concatenate([[0], np.cumsum(nv)]).astype(np.int64)
+    soff = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+    xv = np.zeros((max(int(voff[-1]), 1), 3))
+    xs = np.zeros((max(int(soff[-1]), 1), 3))
+    fvals = gvals = None
+    if forcing is not None or (nitsche and dirichlet is not None):
+        lib.cutcell_setup_load_points(C.byref(d), voff.ctypes.data, soff.ctypes.data, xv.ctypes.data, xs.ctypes.data)
+        if forcing is not None:
+            fvals = np.ascontiguousarray(forcing(xv[:, 0], xv[:, 1], xv[:, 2]), dtype=float)
+        if nitsche and dirichlet is not None:
+            gvals = np.ascontiguousarray(dirichlet(xs[:, 0], xs[:, 1], xs[:, 2]), dtype=float)
+    P = (p + 1) ** 3
+    blocks = np.zeros((nc, P, P))
+    mdiag = np.zeros((nc, P))
+    vols = np.zeros(nc)
+    cload = np.zeros((nc, P))
+    rc = lib.cutcell_setup_blocks(
+        C.byref(d), voff.ctypes.data, soff.ctypes.data,
+        None if fvals is None else fvals.ctypes.data, None if gvals is None else gvals.ctypes.data,
+        blocks.ctypes.data, mdiag.ctypes.data, vols.ctypes.data, cload.ctypes.data,
+    )
+    if rc:
+        raise RuntimeError("cutcell_setup_blocks failed")
+    keep = vols > 0.0
+    return blocks, mdiag, vols, cload, keep

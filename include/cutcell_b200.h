@@ -63,25 +63,30 @@ typedef struct {
 typedef struct {
     int32_t n_elements;    /* per axis */
     int32_t degree;
-    int32_t tile;          /* elements per tile edge */
+    int32_t tile;          /* elements per tile edge (4) */
     int32_t n_tiles_axis;
-    int32_t n_tile_list;   /* number of nonempty tiles */
+    int32_t n_items;       /* work items: nonempty tiles and cut-element chunks */
+    int32_t cut_chunk;     /* cut elements per work item */
     int32_t n_cut;
     int32_t n_full;        /* (n_elements+degree)^3 */
     int32_t n_red;
     int32_t n_small;
     double a_mass;
-    const int32_t* tile_list;  /* [n_tile_list] linear tile ids */
+    const int32_t* item_list;  /* [n_items] >= 0: tile id, < 0: cut chunk -(k+1); heaviest first */
     const int32_t* tile_kind;  /* [n_tiles_axis^3] 0 empty, 1 full, 2 mixed */
-    const int32_t* tile_eptr;  /* [n_tiles_axis^3 + 1] */
+    const int32_t* tile_eptr;  /* [n_tiles_axis^3 + 1] uncut elements of mixed tiles */
     const int32_t* tile_elem;  /* local element id (ez*tile+ey)*tile+ex */
-    const int32_t* tile_ecut;  /* cut block index or -1 */
+    const int32_t* tile_ecut;  /* reserved (cut elements are separate work items) */
     const double* M1;          /* [n][(p+1)^2] */
     const double* Kt1;         /* [3][n][(p+1)^2] */
     const double* TM;          /* [n_tiles_axis][D^2], D = tile+degree */
     const double* TA;          /* [n_tiles_axis][D^2] */
     const double* TK;          /* [3][n_tiles_axis][D^2] */
     const double* cut_mats;    /* [n_cut][(p+1)^6] */
+    const int32_t* cut_base;   /* [n_cut] full index of each cut element's first DOF */
+    const int32_t* cut_dof_slot; /* [n_full] slot in the DOF -> cut-element list, -1 if none */
+    const int32_t* cut_dof_ptr;  /* [n_slots + 1] */
+    const int32_t* cut_dof_ent;  /* cut * (p+1)^3 + local row, ascending per slot */
     const int32_t* red_of_full;
     const int32_t* small_slot;
     const int32_t* small_ptr;

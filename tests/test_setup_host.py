@@ -135,22 +135,33 @@ def test_device_layout_reproduces_E():
 
 @pytest.mark.parametrize("kind,n,p", [("sphere", 6, 2), ("plane", 6, 3), ("sphere", 9, 3)])
 def test_tile_layout_reproduces_operator(kind, n, p):
-    """Host emulation of the device tile apply equals the oracle's E^T A E."""
+    """Host emulation of the device work items (full tiles, uncut elements of
+    mixed tiles, cut-element chunks + the DOF -> cut lists) equals E^T A E."""
     prob, ext, A_full, A_red, b = system(kind, n, p)
     lay = build_tile_layout(prob, 4)
     T, nta, D = lay.tile, lay.n_tiles_axis, lay.tile + p
     nb = n + p
+    P = prob.P
     rng = np.random.default_rng(1)
     x = rng.standard_normal(ext.n_red)
     xf = ext.E @ x
     yf = np.zeros(ext.n_full)
-    cut_pos = {int(c): k for k, c in enumerate(prob.cut_ids)}
     seen = np.zeros((n, n, n), dtype=int)
-    for t in lay.tile_list:
+    ycut = np.zeros((prob.cut_ids.size, P))
+    for code in lay.item_list:
+        if code < 0:
+            k = -code - 1
+            for c in range(k * lay.cut_chunk, min((k + 1) * lay.cut_chunk, prob.cut_ids.size)):
+                base = lay.cut_base[c]
+                ez, ey, ex = np.unravel_index(prob.cut_ids[c], (n, n, n))
+                assert base == (ez * nb + ey) * nb + ex
+                R = prob.element_rows(ex, ey, ez)[0]
+                ycut[c] = prob.cut_mats[c] @ xf[R]
+                seen[ez, ey, ex] += 1
+            continue
+        t = code
         tz, ty, tx = t // (nta * nta), (t // nta) % nta, t % nta
-        kind_t = lay.tile_kind[t]
-        assert kind_t in (TILE_FULL, TILE_MIXED)
-        if kind_t == TILE_FULL:
+        if lay.tile_kind[t] == TILE_FULL:
             g = [np.arange(tt * T, tt * T + D) for tt in (tx, ty, tz)]
             rows = ((g[2][:, None] * nb + g[1][None, :])[:, :, None] * nb + g[0][None, None, :]).reshape(-1)
             B = (
@@ -161,20 +172,22 @@ def test_tile_layout_reproduces_operator(kind, n, p):
             yf[rows] += B @ xf[rows]
             seen[tz * T : tz * T + T, ty * T : ty * T + T, tx * T : tx * T + T] += 1
         else:
+            assert lay.tile_kind[t] == TILE_MIXED
             for it in range(lay.tile_eptr[t], lay.tile_eptr[t + 1]):
                 le = lay.tile_elem[it]
                 lx, ly, lz = le % T, (le // T) % T, le // (T * T)
                 ex, ey, ez = tx * T + lx, ty * T + ly, tz * T + lz
+                assert prob.elem_type[ez, ey, ex] == FULL
                 R = prob.element_rows(ex, ey, ez)[0]
-                c = lay.tile_ecut[it]
-                if c >= 0:
-                    assert cut_pos[(ez * n + ey) * n + ex] == c
-                    B = prob.cut_mats[c]
-                else:
-                    B = prob.full_element_blocks(np.array([ex]), np.array([ey]), np.array([ez]))[0]
+                B = prob.full_element_blocks(np.array([ex]), np.array([ey]), np.array([ez]))[0]
                 yf[R] += B @ xf[R]
                 seen[ez, ey, ex] += 1
     assert np.array_equal(seen, (prob.elem_type != 0).astype(int))
+    # cut partials through the DOF -> cut lists
+    for g in np.nonzero(lay.cut_dof_slot >= 0)[0]:
+        s_ = lay.cut_dof_slot[g]
+        for e in lay.cut_dof_ent[lay.cut_dof_ptr[s_] : lay.cut_dof_ptr[s_ + 1]]:
+            yf[g] += ycut[e // P, e % P]
     y = ext.E.T @ yf
     ref = A_red @ x
     np.testing.assert_allclose(y, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
@@ -185,3 +198,19 @@ def test_jacobi_diagonal(kind, n, p):
     prob, ext, A_full, A_red, b = system(kind, n, p)
     d = jacobi_diagonal(prob, ext)
     np.testing.assert_allclose(d, A_red.diagonal(), rtol=1e-12)
+
+
+@pytest.mark.parametrize("kind", ["sphere", "plane"])
+def test_native_setup_matches_python(kind):
+    from cutcell_b200.problem import _setup_lib, manufactured_sine
+
+    assert _setup_lib() is not None, "libcutcell_setup.so not built"
+    u, f = manufactured_sine()
+    phi = sphere() if kind == "sphere" else plane5()
+    a = build_problem(phi, 6, 3, forcing=f, dirichlet=u, native=False)
+    b = build_problem(phi, 6, 3, forcing=f, dirichlet=u, native=True)
+    assert np.array_equal(a.cut_ids, b.cut_ids)
+    np.testing.assert_allclose(b.cut_mats, a.cut_mats, rtol=0, atol=1e-13 * np.abs(a.cut_mats).max())
+    np.testing.assert_allclose(b.load, a.load, rtol=0, atol=1e-13 * np.abs(a.load).max())
+    np.testing.assert_allclose(b.gamma, a.gamma, rtol=0, atol=1e-13)
+    np.testing.assert_allclose(b.cut_fractions, a.cut_fractions, rtol=0, atol=1e-14)
