@@ -100,6 +100,7 @@ struct cutcell_ctx {
     __nv_bfloat16* cut16 = nullptr;
     double* ypart = nullptr;
     double* ycut = nullptr;
+    double* yfv = nullptr;
     // scratch
     double* dinv = nullptr;
     double* ones = nullptr;
@@ -319,6 +320,8 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     CK(cudaMemset(c->ypart, 0, nt3 * D * D * D * sizeof(double)));
     CK(cudaMalloc(&c->ycut, ((size_t)t->n_cut * P + 1) * sizeof(double)));
     CK(cudaMemset(c->ycut, 0, ((size_t)t->n_cut * P + 1) * sizeof(double)));
+    CK(cudaMalloc(&c->yfv, (size_t)t->n_full * sizeof(double)));
+    CK(cudaMemset(c->yfv, 0, (size_t)t->n_full * sizeof(double)));
     const size_t ncm = (size_t)t->n_cut * P * P;
     if (ncm) {
         CK(cudaMalloc(&c->cut32, ncm * sizeof(float)));
@@ -366,6 +369,9 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     d.ext = e;
     d.ypart = c->ypart;
     d.ycut = c->ycut;
+    d.yfv = c->yfv;
+    d.need = t->need;
+    d.n_need = t->n_need;
     d.work = c->bar + 3;
     c->cut64 = t->cut_mats;
     diag_inv_kernel<<<ceil_div(t->n_red, 256), 256>>>(t->n_red, t->diag, c->dinv);
@@ -476,7 +482,7 @@ int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
-    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->yfv, c->dinv, c->ones, c->r,
                     c->p,     c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);

@@ -131,6 +131,9 @@ struct TileData {
     ExtDev ext;
     double* ypart;             // [nta^3][D^3]
     double* ycut;              // [n_cut][P]
+    double* yfv;               // [n_full] full-space values of the needed DOFs
+    const int* need;           // [n_need] full DOFs read by the E^T scatter
+    int n_need;
     unsigned* work;            // dynamic work counter (reset in phase 2)
 };
 
@@ -421,17 +424,29 @@ struct TileOp {
     }
 
     __device__ __forceinline__ double scatter_row(int j) const {
-        double y = yfull(__ldg(td.ext.full_of_red + j));
+        double y = __ldcg(td.yfv + __ldg(td.ext.full_of_red + j));
         const int k1 = __ldg(td.ext.smallT_ptr + j + 1);
-        for (int k = __ldg(td.ext.smallT_ptr + j); k < k1; ++k)
-            y += __ldg(td.ext.smallT_val + k) * yfull(__ldg(td.ext.smallT_row + k));
-        return y;
+        int k = __ldg(td.ext.smallT_ptr + j);
+        double y2 = 0.0;
+        for (; k + 1 < k1; k += 2) {
+            y += __ldg(td.ext.smallT_val + k) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k));
+            y2 += __ldg(td.ext.smallT_val + k + 1) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k + 1));
+        }
+        if (k < k1) y += __ldg(td.ext.smallT_val + k) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k));
+        return y + y2;
     }
 
+    // phase 2a: full-space values of the DOFs the scatter reads; phase 2b:
+    // y = E^T yf and the partial of p.y.
     __device__ __forceinline__ double apply(const double* p, double* y, const GridSync& gs, double* sm) const {
         phase1(p, sm);
         if (!grid_sync(gs)) return 0.0;
         if (blockIdx.x == 0 && threadIdx.x == 0) *td.work = 0u;  // every block has left phase 1
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < td.n_need; k += gridDim.x * blockDim.x) {
+            const int i = __ldg(td.need + k);
+            td.yfv[i] = yfull(i);
+        }
+        if (!grid_sync(gs)) return 0.0;
         double part = 0.0;
         for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < td.ext.n_red; j += gridDim.x * blockDim.x) {
             const double yj = scatter_row(j);

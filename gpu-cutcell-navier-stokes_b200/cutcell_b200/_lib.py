@@ -64,6 +64,7 @@ class CutcellTileDesc(C.Structure):
         ("n_full", C.c_int32),
         ("n_red", C.c_int32),
         ("n_small", C.c_int32),
+        ("n_need", C.c_int32),
         ("a_mass", C.c_double),
         ("item_list", _P),
         ("tile_kind", _P),
@@ -80,6 +81,7 @@ class CutcellTileDesc(C.Structure):
         ("cut_dof_slot", _P),
         ("cut_dof_ptr", _P),
         ("cut_dof_ent", _P),
+        ("need", _P),
         ("red_of_full", _P),
         ("small_slot", _P),
         ("small_ptr", _P),

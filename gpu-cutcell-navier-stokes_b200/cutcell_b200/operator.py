@@ -211,6 +211,8 @@ class CutCellOperator:
         t["cut_dof_slot"] = _dev(lay.cut_dof_slot, i32, dv)
         t["cut_dof_ptr"] = _dev(lay.cut_dof_ptr, i32, dv)
         t["cut_dof_ent"] = _dev(np.append(lay.cut_dof_ent, 0), i32, dv)
+        need = np.union1d(np.asarray(ext.interior), np.asarray(ext.small_support)).astype(np.int32)
+        t["need"] = _dev(need, i32, dv)
         t["M1"] = _dev(prob.M1, f64, dv)
         t["Kt1"] = _dev(prob.Kt1, f64, dv)
         t["TM"] = _dev(lay.TM, f64, dv)
@@ -236,6 +238,7 @@ class CutCellOperator:
         desc.n_full = prob.n_full
         desc.n_red = ext.n_red
         desc.n_small = int(ext.small_support.size)
+        desc.n_need = int(need.size)
         desc.a_mass = prob.a_mass
         for name, _ in _lib.CutcellTileDesc._fields_:
             if name in t:

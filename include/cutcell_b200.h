@@ -71,6 +71,7 @@ typedef struct {
     int32_t n_full;        /* (n_elements+degree)^3 */
     int32_t n_red;
     int32_t n_small;
+    int32_t n_need;        /* full DOFs read by the E^T scatter (identity + small rows) */
     double a_mass;
     const int32_t* item_list;  /* [n_items] >= 0: tile id, < 0: cut chunk -(k+1); heaviest first */
     const int32_t* tile_kind;  /* [n_tiles_axis^3] 0 empty, 1 full, 2 mixed */
@@ -87,6 +88,7 @@ typedef struct {
     const int32_t* cut_dof_slot; /* [n_full] slot in the DOF -> cut-element list, -1 if none */
     const int32_t* cut_dof_ptr;  /* [n_slots + 1] */
     const int32_t* cut_dof_ent;  /* cut * (p+1)^3 + local row, ascending per slot */
+    const int32_t* need;         /* [n_need] full DOF indices */
     const int32_t* red_of_full;
     const int32_t* small_slot;
     const int32_t* small_ptr;
