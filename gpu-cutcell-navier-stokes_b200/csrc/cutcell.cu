@@ -101,6 +101,7 @@ struct cutcell_ctx {
     double* ypart = nullptr;
     double* ycut = nullptr;
     double* yfv = nullptr;
+    double* psmall = nullptr;
     // scratch
     double* dinv = nullptr;
     double* ones = nullptr;
@@ -321,6 +322,7 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     CK(cudaMalloc(&c->ycut, ((size_t)t->n_cut * P + 1) * sizeof(double)));
     CK(cudaMemset(c->ycut, 0, ((size_t)t->n_cut * P + 1) * sizeof(double)));
     CK(cudaMalloc(&c->yfv, (size_t)t->n_full * sizeof(double)));
+    CK(cudaMalloc(&c->psmall, ((size_t)t->n_small + 1) * sizeof(double)));
     CK(cudaMemset(c->yfv, 0, (size_t)t->n_full * sizeof(double)));
     const size_t ncm = (size_t)t->n_cut * P * P;
     if (ncm) {
@@ -342,6 +344,7 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     e.smallT_ptr = t->smallT_ptr;
     e.smallT_row = t->smallT_row;
     e.smallT_val = t->smallT_val;
+    e.psmall = c->psmall;
     TileData& d = c->td;
     d.n = t->n_elements;
     d.p = p;
@@ -373,6 +376,7 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     d.need = t->need;
     d.n_need = t->n_need;
     d.work = c->bar + 3;
+    d.work2 = c->bar + 6;
     c->cut64 = t->cut_mats;
     diag_inv_kernel<<<ceil_div(t->n_red, 256), 256>>>(t->n_red, t->diag, c->dinv);
     CK(cudaGetLastError());
@@ -482,7 +486,7 @@ int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
-    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->yfv, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->yfv, c->psmall, c->dinv, c->ones, c->r,
                     c->p,     c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);

@@ -72,6 +72,29 @@ struct ExtDev {
     const int* __restrict__ smallT_ptr;    // [n_red+1]  E_small^T rows
     const int* __restrict__ smallT_row;    // full index of the contributing small row
     const double* __restrict__ smallT_val;
+    double* psmall;                        // [n_small] (E x) on the small rows, refreshed per apply
+
+    // warp-cooperative values of the small rows: psmall[s] = E[small s, :] x
+    __device__ __forceinline__ void small_rows(const double* x) const {
+        const int lane = threadIdx.x & 31;
+        const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const int nw = (gridDim.x * blockDim.x) >> 5;
+        for (int s = gw; s < n_small; s += nw) {
+            double acc = 0.0;
+            const int k1 = __ldg(small_ptr + s + 1);
+            for (int k = __ldg(small_ptr + s) + lane; k < k1; k += 32) acc += __ldg(small_val + k) * __ldcg(x + __ldg(small_idx + k));
+            acc = warp_sum(acc);
+            if (lane == 0) psmall[s] = acc;
+        }
+    }
+
+    // (E x)_i once small_rows(x) has completed grid-wide
+    __device__ __forceinline__ double gather_fast(const double* x, int i) const {
+        const int r = __ldg(red_of_full + i);
+        if (r >= 0) return __ldcg(x + r);
+        const int s = __ldg(small_slot + i);
+        return s >= 0 ? __ldcg(psmall + s) : 0.0;
+    }
 
     // (E x)_i
     __device__ __forceinline__ double gather(const double* x, int i) const {
@@ -134,7 +157,8 @@ struct TileData {
     double* yfv;               // [n_full] full-space values of the needed DOFs
     const int* need;           // [n_need] full DOFs read by the E^T scatter
     int n_need;
-    unsigned* work;            // dynamic work counter (reset in phase 2)
+    unsigned* work;            // dynamic tile-item counter (reset in phase 2)
+    unsigned* work2;           // dynamic cut-element counter, claimed per warp
 };
 
 template <typename CT, int P1>
@@ -155,7 +179,7 @@ struct TileOp {
     static size_t smem_bytes() {
         const size_t full = 5 * (size_t)D3a;
         const size_t mixed = (size_t)D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa + 3 * 4 * 2 * PP;
-        const size_t cut = (size_t)Pa;
+        const size_t cut = (size_t)NW * Pa;
         size_t m = full > mixed ? full : mixed;
         return (CTRL + (m > cut ? m : cut)) * sizeof(double);
     }
@@ -166,7 +190,7 @@ struct TileOp {
             const int dx = k % D, dy = (k / D) % D, dz = k / (D * D);
             const int gx = tx * T + dx, gy = ty * T + dy, gz = tz * T + dz;
             double v = 0.0;
-            if (gx < nb && gy < nb && gz < nb) v = td.ext.gather(pred, (gz * nb + gy) * nb + gx);
+            if (gx < nb && gy < nb && gz < nb) v = td.ext.gather_fast(pred, (gz * nb + gy) * nb + gx);
             xs[k] = v;
         }
     }
@@ -313,36 +337,37 @@ struct TileOp {
         }
     }
 
-    // one cut element: x_e gathered through E, y_e = A_e x_e -> ycut[c]
-    __device__ void cut_element(const double* pred, int c, double* xe) const {
+    // one cut element per warp: x_e gathered through E into the warp's
+    // shared slice, y_e = A_e x_e with lane-owned rows (A_e symmetric, so
+    // column c of the row-major block is row c: for fixed c the 32 lanes read
+    // 32 consecutive entries), ceil(P/32) independent accumulators per lane.
+    static constexpr int RPL = (P + 31) / 32;
+    __device__ void cut_element_warp(const double* pred, int c, double* xe) const {
         typedef typename Conv<CT>::acc acc_t;
+        const int lane = threadIdx.x & 31;
         const int nb = td.nb;
         const int base = __ldg(td.cut_base + c);
-        for (int k = threadIdx.x; k < P; k += blockDim.x) {
+        for (int k = lane; k < P; k += 32) {
             const int a = k % P1, b = (k / P1) % P1, cc = k / PP;
-            xe[k] = td.ext.gather(pred, base + (cc * nb + b) * nb + a);
+            xe[k] = td.ext.gather_fast(pred, base + (cc * nb + b) * nb + a);
         }
-        __syncthreads();
+        __syncwarp();
         const CT* A = cut_mats + (size_t)c * P * P;
-        const int q = threadIdx.x & 3;
-        if (!CUTCELL_OK_IF(CUTCELL_ALIGNED(A, sizeof(CT)) && c < td.n_cut, 11, c, td.work + 1)) {
-            __syncthreads();
-            return;
-        }
-        for (int r0 = 0; r0 < P; r0 += (int)(blockDim.x >> 2)) {
-            const int r = r0 + (int)(threadIdx.x >> 2);
-            acc_t s = 0;
-            if (r < P) {
-                const CT* Ar = A + (size_t)r * P;
+        acc_t acc[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) acc[q] = 0;
 #pragma unroll 8
-                for (int col = q; col < P; col += 4) s += Conv<CT>::ld(Ar + col) * (acc_t)xe[col];
-            }
-            s += __shfl_xor_sync(0xffffffffu, s, 1);
-            s += __shfl_xor_sync(0xffffffffu, s, 2);
-            if (r < P && q == 0 && CUTCELL_OK_IF(CUTCELL_ALIGNED(td.ycut + (size_t)c * P + r, 8), 12, r, td.work + 1))
-                td.ycut[(size_t)c * P + r] = (double)s;
+        for (int col = 0; col < P; ++col) {
+            const acc_t xv = (acc_t)xe[col];
+            const CT* Ac = A + (size_t)col * P + lane;
+#pragma unroll
+            for (int q = 0; q < RPL; ++q)
+                if (lane + 32 * q < P) acc[q] += Conv<CT>::ld(Ac + 32 * q) * xv;
         }
-        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < RPL; ++q)
+            if (lane + 32 * q < P) td.ycut[(size_t)c * P + lane + 32 * q] = (double)acc[q];
+        __syncwarp();
     }
 
     __device__ void phase1(const double* pred, double* smem) const {
@@ -387,71 +412,94 @@ struct TileOp {
                 else
                     mixed_tile(tile, tx, ty, tz, xs, out);
                 __syncthreads();
-            } else {
-                const int c0 = (-code - 1) * td.cut_chunk;
-                const int c1 = min(c0 + td.cut_chunk, td.n_cut);
-                if (!CUTCELL_OK_IF(c0 >= 0 && c0 < td.n_cut, 10, c0, td.work + 1)) continue;
-                for (int c = c0; c < c1; ++c) cut_element(pred, c, sm);
             }
         }
+        // cut elements, one per warp, claimed warp by warp
+        const int lane = threadIdx.x & 31;
+        double* xe = sm + (size_t)(threadIdx.x >> 5) * Pa;
+        while (true) {
+            int c = 0;
+            if (lane == 0) c = (int)atomicAdd(td.work2, 1u);
+            c = __shfl_sync(0xffffffffu, c, 0);
+            if (c >= td.n_cut) break;
+            cut_element_warp(pred, c, xe);
+        }
+        __syncthreads();
     }
 
-    __device__ __forceinline__ double yfull(int i) const {
+    // full-space value of DOF i, summed by the 4 lanes q = 0..3 of a group
+    // (tile partials and cut-element partials interleaved over the lanes,
+    // then a fixed xor tree): every lane returns the same bits.
+    __device__ __forceinline__ double yfull4(int i, int q) const {
         const int nb = td.nb, nta = td.nta;
         const int ix = i % nb, iy = (i / nb) % nb, iz = i / (nb * nb);
         const int t1x = min(ix / T, nta - 1), t1y = min(iy / T, nta - 1), t1z = min(iz / T, nta - 1);
         double s = 0.0;
-        for (int tz = t1z - 1; tz <= t1z; ++tz) {
-            if (tz < 0 || iz - tz * T >= D) continue;
-            for (int ty = t1y - 1; ty <= t1y; ++ty) {
-                if (ty < 0 || iy - ty * T >= D) continue;
-                for (int tx = t1x - 1; tx <= t1x; ++tx) {
-                    if (tx < 0 || ix - tx * T >= D) continue;
-                    const int tile = (tz * nta + ty) * nta + tx;
-                    s += __ldcg(td.ypart + (size_t)tile * D3 + ((iz - tz * T) * D + (iy - ty * T)) * D + (ix - tx * T));
-                }
-            }
+        // candidate tiles: 8 combinations, lane q takes combinations q and q+4
+        for (int m = q; m < 8; m += 4) {
+            const int tz = t1z - ((m >> 2) & 1), ty = t1y - ((m >> 1) & 1), tx = t1x - (m & 1);
+            if (tz < 0 || ty < 0 || tx < 0) continue;
+            if (iz - tz * T >= D || iy - ty * T >= D || ix - tx * T >= D) continue;
+            const int tile = (tz * nta + ty) * nta + tx;
+            s += __ldcg(td.ypart + (size_t)tile * D3 + ((iz - tz * T) * D + (iy - ty * T)) * D + (ix - tx * T));
         }
         const int slot = __ldg(td.cut_dof_slot + i);
         if (slot >= 0) {
             const int k1 = __ldg(td.cut_dof_ptr + slot + 1);
-            for (int k = __ldg(td.cut_dof_ptr + slot); k < k1; ++k) {
+            for (int k = __ldg(td.cut_dof_ptr + slot) + q; k < k1; k += 4) {
                 const int e = __ldg(td.cut_dof_ent + k);
                 if (CUTCELL_OK_IF(e >= 0 && e < td.n_cut * P, 13, e, td.work + 1)) s += __ldcg(td.ycut + e);
             }
         }
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
         return s;
     }
 
-    __device__ __forceinline__ double scatter_row(int j) const {
-        double y = __ldcg(td.yfv + __ldg(td.ext.full_of_red + j));
+    __device__ __forceinline__ double scatter_row4(int j, int q) const {
+        double y = (q == 0) ? __ldcg(td.yfv + __ldg(td.ext.full_of_red + j)) : 0.0;
         const int k1 = __ldg(td.ext.smallT_ptr + j + 1);
-        int k = __ldg(td.ext.smallT_ptr + j);
-        double y2 = 0.0;
-        for (; k + 1 < k1; k += 2) {
+        for (int k = __ldg(td.ext.smallT_ptr + j) + q; k < k1; k += 4)
             y += __ldg(td.ext.smallT_val + k) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k));
-            y2 += __ldg(td.ext.smallT_val + k + 1) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k + 1));
-        }
-        if (k < k1) y += __ldg(td.ext.smallT_val + k) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k));
-        return y + y2;
+        y += __shfl_xor_sync(0xffffffffu, y, 1);
+        y += __shfl_xor_sync(0xffffffffu, y, 2);
+        return y;
     }
 
+    // phase 0: small-row values of E p; phase 1: tiles and cut elements;
     // phase 2a: full-space values of the DOFs the scatter reads; phase 2b:
-    // y = E^T yf and the partial of p.y.
+    // y = E^T yf and the partial of p.y.  Groups of 4 lanes own one DOF/row.
     __device__ __forceinline__ double apply(const double* p, double* y, const GridSync& gs, double* sm) const {
+        td.ext.small_rows(p);
+        if (!grid_sync(gs)) return 0.0;
         phase1(p, sm);
         if (!grid_sync(gs)) return 0.0;
-        if (blockIdx.x == 0 && threadIdx.x == 0) *td.work = 0u;  // every block has left phase 1
-        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < td.n_need; k += gridDim.x * blockDim.x) {
-            const int i = __ldg(td.need + k);
-            td.yfv[i] = yfull(i);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {  // every block has left phase 1
+            *td.work = 0u;
+            *td.work2 = 0u;
+        }
+        const int q = threadIdx.x & 3;
+        const int g0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+        const int ng = (gridDim.x * blockDim.x) >> 2;
+        const int nneed = td.n_need;
+        for (int kb = g0 - (g0 & 7); kb < nneed; kb += ng) {  // warp-uniform trip count
+            const int k = kb + (g0 & 7);
+            const bool ok = k < nneed;
+            const int i = ok ? __ldg(td.need + k) : 0;
+            const double v = yfull4(i, q);
+            if (ok && q == 0) td.yfv[i] = v;
         }
         if (!grid_sync(gs)) return 0.0;
         double part = 0.0;
-        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < td.ext.n_red; j += gridDim.x * blockDim.x) {
-            const double yj = scatter_row(j);
-            y[j] = yj;
-            part += __ldcg(p + j) * yj;
+        const int nred = td.ext.n_red;
+        for (int jb = g0 - (g0 & 7); jb < nred; jb += ng) {
+            const int j = jb + (g0 & 7);
+            const bool ok = j < nred;
+            const double yj = scatter_row4(ok ? j : 0, q);
+            if (ok && q == 0) {
+                y[j] = yj;
+                part += __ldcg(p + j) * yj;
+            }
         }
         return part;
     }

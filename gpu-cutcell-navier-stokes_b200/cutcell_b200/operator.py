@@ -81,10 +81,11 @@ def build_tile_layout(prob: CutCellProblem, tile: int = 4, cut_chunk: int = 2) -
     tile_elem = np.concatenate(elems) if elems else np.zeros(0, np.int32)
     ncut = int(prob.cut_ids.size)
     nchunk = -(-ncut // cut_chunk)
-    # work order: heaviest mixed tiles, cut chunks, then full tiles
+    # work order: heaviest mixed tiles, then full tiles
     mixed = sorted(mixed_cost, key=lambda t: (-mixed_cost[t], t))
     full = [int(t) for t in np.nonzero(kind == TILE_FULL)[0]]
-    item_list = np.array(mixed + [-(k + 1) for k in range(nchunk)] + full, dtype=np.int32)
+    # cut elements are claimed warp by warp after the tiles (not tile items)
+    item_list = np.array(mixed + full, dtype=np.int32)
     # tile-assembled 1D factors
     TM = np.zeros((nta, D, D))
     TK = np.zeros((3, nta, D, D))

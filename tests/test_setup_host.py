@@ -148,6 +148,13 @@ def test_tile_layout_reproduces_operator(kind, n, p):
     yf = np.zeros(ext.n_full)
     seen = np.zeros((n, n, n), dtype=int)
     ycut = np.zeros((prob.cut_ids.size, P))
+    for c in range(prob.cut_ids.size):
+        base = lay.cut_base[c]
+        ez, ey, ex = np.unravel_index(prob.cut_ids[c], (n, n, n))
+        assert base == (ez * nb + ey) * nb + ex
+        R = prob.element_rows(ex, ey, ez)[0]
+        ycut[c] = prob.cut_mats[c] @ xf[R]
+        seen[ez, ey, ex] += 1
     for code in lay.item_list:
         if code < 0:
             k = -code - 1
