@@ -18,9 +18,9 @@
 #define CUTCELL_BARRIER_CYCLES 2000000000LL
 
 struct GridSync {
-    unsigned* count;
-    unsigned* gen;
-    int* err;
+    unsigned* count;  // arrival word (own 128-byte line); its top bit flips once per barrier
+    unsigned* gen;    // unused (kept for layout compatibility)
+    int* err;         // error word (own 128-byte line)
     unsigned nblocks;
 };
 
@@ -28,28 +28,32 @@ __device__ __forceinline__ int grid_error(const GridSync& gs) {
     return *((volatile int*)gs.err);
 }
 
-// Sense-free generation barrier for a cooperative (co-resident) grid.  Every
-// wait is bounded; on timeout the error word is set and the caller returns.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid barrier for a cooperative (co-resident) grid: every block adds to one
+// arrival word, block 0 adds 2^31 - (nblocks - 1) so the word's top bit flips
+// exactly when the last block arrives; waiters poll the word with acquire
+// loads.  No reset is needed between barriers.  Every wait is bounded: after
+// CUTCELL_BARRIER_CYCLES the error word is set and all blocks leave their loops.
 __device__ __forceinline__ bool grid_sync(const GridSync& gs) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned* vgen = gs.gen;
-        unsigned g = *vgen;
+        const unsigned add = (blockIdx.x == 0) ? (0x80000000u - (gs.nblocks - 1u)) : 1u;
         __threadfence();
-        unsigned arrived = atomicAdd(gs.count, 1u);
-        if (arrived == gs.nblocks - 1) {
-            atomicExch(gs.count, 0u);
-            __threadfence();
-            atomicAdd(gs.gen, 1u);
-        } else {
-            long long t0 = clock64();
-            while (*vgen == g) {
+        const unsigned old = atomicAdd(gs.count, add);
+        long long t0 = clock64();
+        unsigned spins = 0;
+        while (((old ^ ld_acquire_u32(gs.count)) & 0x80000000u) == 0u) {
+            if ((++spins & 1023u) == 0u) {
                 if (clock64() - t0 > CUTCELL_BARRIER_CYCLES) {
                     atomicExch(gs.err, CUTCELL_E_BARRIER);
                     break;
                 }
                 if (*((volatile int*)gs.err) != 0) break;
-                __nanosleep(32);
             }
         }
         __threadfence();

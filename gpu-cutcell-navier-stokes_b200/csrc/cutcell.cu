@@ -22,6 +22,7 @@ int cuda_fail(cudaError_t e, const char* what) {
     } while (0)
 
 enum { KIND_CSR = 0, KIND_TILES = 1 };
+constexpr int BAR_WORDS = 160;
 
 __global__ void csr_diag_inv_kernel(int n, const int* ptr, const int* idx, const double* val, double* dinv) {
     for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
@@ -112,7 +113,7 @@ struct cutcell_ctx {
     double* d = nullptr;
     double* rhat = nullptr;
     double* part = nullptr;
-    unsigned* bar = nullptr;  // [0] count, [1] gen, [2] err (int)
+    unsigned* bar = nullptr;  // control words, one 128-byte line each: [0] arrival, [32] err, [64] tile work, [96] cut work, [128..] debug
     DevResult* res = nullptr;
     int max_blocks = 0;
     // refinement
@@ -132,7 +133,7 @@ static int alloc_scratch(cutcell_ctx* c) {
     CK(cudaMalloc(&c->Ap, nb));
     CK(cudaMalloc(&c->d, nb));
     CK(cudaMalloc(&c->rhat, nb));
-    CK(cudaMalloc(&c->bar, 8 * sizeof(unsigned)));
+    CK(cudaMalloc(&c->bar, BAR_WORDS * sizeof(unsigned)));
     CK(cudaMalloc(&c->res, sizeof(DevResult)));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
@@ -155,8 +156,8 @@ static int ensure_part(cutcell_ctx* c, K kernel, size_t smem, int* blocks) {
 static GridSync make_gs(cutcell_ctx* c, int blocks) {
     GridSync gs;
     gs.count = c->bar;
-    gs.gen = c->bar + 1;
-    gs.err = (int*)(c->bar + 2);
+    gs.gen = c->bar;
+    gs.err = (int*)(c->bar + 32);
     gs.nblocks = (unsigned)blocks;
     return gs;
 }
@@ -206,7 +207,7 @@ static int run_apply(cutcell_ctx* c, const Op& op, size_t smem, const double* x,
     int blocks = 0;
     int st = ensure_part(c, kern, smem, &blocks);
     if (st) return st;
-    CK(cudaMemsetAsync(c->bar, 0, 8 * sizeof(unsigned), s));
+    CK(cudaMemsetAsync(c->bar, 0, BAR_WORDS * sizeof(unsigned), s));
     GridSync gs = make_gs(c, blocks);
     return launch_coop(kern, blocks, smem, s, op, x, y, gs);
 }
@@ -375,8 +376,8 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     d.yfv = c->yfv;
     d.need = t->need;
     d.n_need = t->n_need;
-    d.work = c->bar + 3;
-    d.work2 = c->bar + 6;
+    d.work = c->bar + 64;
+    d.work2 = c->bar + 96;
     c->cut64 = t->cut_mats;
     diag_inv_kernel<<<ceil_div(t->n_red, 256), 256>>>(t->n_red, t->diag, c->dinv);
     CK(cudaGetLastError());
@@ -413,7 +414,7 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
     a.d = c->d;
     a.rhat = c->rhat;
     a.res = c->res;
-    CK(cudaMemsetAsync(c->bar, 0, 8 * sizeof(unsigned), s));
+    CK(cudaMemsetAsync(c->bar, 0, BAR_WORDS * sizeof(unsigned), s));
     CK(cudaEventRecord(c->ev0, s));
     int blocks = 0;
     int st = CUTCELL_OK;
@@ -431,10 +432,10 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
     CK(cudaEventRecord(c->ev1, s));
 #ifdef CUTCELL_DEBUG_CHECKS
     {
-        unsigned w[8];
+        unsigned w[BAR_WORDS];
         CK(cudaMemcpyAsync(w, c->bar, sizeof(w), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        if (w[4]) fprintf(stderr, "cutcell debug check failed: code %u info %u\n", w[4], w[5]);
+        if (w[128]) fprintf(stderr, "cutcell debug check failed: code %u info %u\n", w[128], w[129]);
     }
 #endif
     DevResult hr;

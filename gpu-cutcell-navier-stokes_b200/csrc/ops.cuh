@@ -374,7 +374,7 @@ struct TileOp {
         int& s_item = *reinterpret_cast<int*>(smem);
         double* sm = smem + CTRL;
 #ifdef CUTCELL_DEBUG_CHECKS
-        unsigned* dbgw = td.work + 1;
+        unsigned* dbgw = (td.work + 64);
         if (threadIdx.x == 0) {
             CUTCELL_OK_IF(CUTCELL_ALIGNED(sm, 16), 1, 0, dbgw);
             CUTCELL_OK_IF(CUTCELL_ALIGNED(cut_mats, sizeof(CT)), 2, 0, dbgw);
@@ -396,12 +396,12 @@ struct TileOp {
             const int item = s_item;
             __syncthreads();
             if (item >= td.n_items) break;
-            if (!CUTCELL_OK_IF(item >= 0, 8, item, td.work + 1)) break;
+            if (!CUTCELL_OK_IF(item >= 0, 8, item, (td.work + 64))) break;
             const int code = __ldg(td.item_list + item);
             if (code >= 0) {
                 const int tile = code;
                 const int nta = td.nta;
-                if (!CUTCELL_OK_IF(tile < nta * nta * nta, 9, tile, td.work + 1)) continue;
+                if (!CUTCELL_OK_IF(tile < nta * nta * nta, 9, tile, (td.work + 64))) continue;
                 const int tx = tile % nta, ty = (tile / nta) % nta, tz = tile / (nta * nta);
                 double* xs = sm;
                 gather_window(pred, tx, ty, tz, xs);
@@ -448,7 +448,7 @@ struct TileOp {
             const int k1 = __ldg(td.cut_dof_ptr + slot + 1);
             for (int k = __ldg(td.cut_dof_ptr + slot) + q; k < k1; k += 4) {
                 const int e = __ldg(td.cut_dof_ent + k);
-                if (CUTCELL_OK_IF(e >= 0 && e < td.n_cut * P, 13, e, td.work + 1)) s += __ldcg(td.ycut + e);
+                if (CUTCELL_OK_IF(e >= 0 && e < td.n_cut * P, 13, e, (td.work + 64))) s += __ldcg(td.ycut + e);
             }
         }
         s += __shfl_xor_sync(0xffffffffu, s, 1);

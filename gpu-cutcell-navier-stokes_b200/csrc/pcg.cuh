@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) ir_kernel(OpHi hi, OpLo lo, 
     const int gstride = gridDim.x * blockDim.x;
 #ifdef CUTCELL_DEBUG_CHECKS
     if (threadIdx.x == 0) {
-        unsigned* w = a.gs.count + 4;
+        unsigned* w = a.gs.count + 128;
         CUTCELL_OK_IF(CUTCELL_ALIGNED(a.x, 8) && CUTCELL_ALIGNED(a.b, 8) && CUTCELL_ALIGNED(a.d, 8) &&
                           CUTCELL_ALIGNED(a.rhat, 8),
                       20, 0, w);
