@@ -6,8 +6,10 @@ sphere-cut Poisson problem (p = 3, 32 elements per axis, r = 0.31), B200.
 One step = one complete solve of the aggregated system E^T A E x = E^T f from
 x = 0 to ||r||/||b|| <= 1e-9, inputs resident in HBM.  The L2 cache (126 MB) is
 flushed between timed solves by writing a 256 MB buffer.  Variants measured:
-plain FP64 Jacobi-PCG (the default form) and FP64 iterative refinement around
-FP32 / BF16 operator applies; ``value`` is the fastest variant that reaches the
+plain FP64 Jacobi-PCG (the default form), FP64 iterative refinement around
+FP32 / BF16 operator applies, and flexible PCG with the learned patch
+correction (trained in this run on random radii in [0.2, 0.4] by the
+project's kernels); ``value`` is the fastest variant that reaches the
 tolerance, every variant is listed under ``variants``.  Multi-GPU: independent
 replicas (one solve per rank per step, no collective on the data path).
 
@@ -47,7 +49,9 @@ def parse():
     ap.add_argument("--p", type=int, default=3)
     ap.add_argument("--radius", type=float, default=0.31)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--variants", default="fp64,fp32-ir,bf16-ir")
+    ap.add_argument("--variants", default="fp64,fp32-ir,bf16-ir,learned")
+    ap.add_argument("--train-geometries", type=int, default=3)
+    ap.add_argument("--train-pairs", type=int, default=20000)
     return ap.parse_args()
 
 
@@ -221,11 +225,32 @@ def main():
 
     variants = {}
     ref_x = None
-    for prec in args.variants.split(","):
-        if prec != "fp64":
+    learned_info = None
+    wanted = args.variants.split(",")
+    if "learned" in wanted:
+        # training on random sphere radii in [0.2, 0.4] with the project's kernels
+        from cutcell_b200.learned import PatchMLP, attach, generate_pairs, train
+
+        t0 = time.perf_counter()
+        rng = np.random.default_rng(20260629)
+        radii = [float(r) for r in rng.uniform(0.2, 0.4, args.train_geometries)]
+        train_ops = [CutCellOperator(*sphere_poisson(args.n, args.p, r), device=dev) for r in radii]
+        X, T = generate_pairs(train_ops, args.train_pairs, seed=11)
+        net = PatchMLP(seed=2)
+        hist = train(net, X, T, epochs=40, batch=512, lr=1e-3)
+        attach(op, net)
+        for o in train_ops:
+            o.close()
+        learned_info = {"radii": radii, "pairs": int(X.shape[0]), "loss_first": hist[0], "loss_last": hist[-1],
+                        "train_s": time.perf_counter() - t0}
+    for prec in wanted:
+        solve_kw = {"precision": prec}
+        if prec == "learned":
+            solve_kw = {"precision": "fp64", "preconditioner": "jacobi+learned"}
+        elif prec != "fp64":
             op.set_refinement(1e-2 if prec == "bf16-ir" else 1e-4)
         for _ in range(args.warmup):
-            x, rep = op.solve_device(b, tol=TOL, maxiter=20000, precision=prec)
+            x, rep = op.solve_device(b, tol=TOL, maxiter=20000, **solve_kw)
         barrier()
         sampler = ClockSampler(local) if prec == "fp64" else None
         if sampler:
@@ -236,7 +261,7 @@ def main():
             barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            x, rep = op.solve_device(b, tol=TOL, maxiter=20000, precision=prec)
+            x, rep = op.solve_device(b, tol=TOL, maxiter=20000, **solve_kw)
             e1.record()
             torch.cuda.synchronize(dev)
             ms.append(e0.elapsed_time(e1))
@@ -264,6 +289,8 @@ def main():
         }
         if clocks:
             variants[prec]["clocks"] = clocks
+        if prec == "learned" and learned_info:
+            variants[prec]["training"] = learned_info
     plain = variants["fp64"]
     ok = {k: v for k, v in variants.items() if v["converged"]}
     best_key = min(ok, key=lambda k: ok[k]["s_per_solve"]) if ok else "fp64"
@@ -272,12 +299,13 @@ def main():
     # end-to-end through the public API, host buffers (pinned), H2D + D2H inside
     b_pin = torch.from_numpy(b_host).pin_memory()
     e2e_prec = best_key
+    e2e_kw = {"precision": e2e_prec} if e2e_prec != "learned" else {"preconditioner": "jacobi+learned"}
     for _ in range(2):
-        solve_spd(op, b_pin.numpy(), tol=TOL, maxiter=20000, precision=e2e_prec)
+        solve_spd(op, b_pin.numpy(), tol=TOL, maxiter=20000, **e2e_kw)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        x_host, rep_h = solve_spd(op, b_pin.numpy(), tol=TOL, maxiter=20000, precision=e2e_prec)
+        x_host, rep_h = solve_spd(op, b_pin.numpy(), tol=TOL, maxiter=20000, **e2e_kw)
     torch.cuda.synchronize(dev)
     e2e = (time.perf_counter() - t0) / args.steps
 

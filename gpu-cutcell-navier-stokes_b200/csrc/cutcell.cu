@@ -5,6 +5,7 @@
 #include <string>
 
 #include "pcg.cuh"
+#include "learned.cuh"
 
 namespace {
 
@@ -84,6 +85,28 @@ int occupancy_blocks(K kernel, size_t smem, int* out) {
 
 }  // namespace
 
+struct cutcell_mlp {
+    int device = 0;
+    float* theta = nullptr;
+    float* m = nullptr;
+    float* v = nullptr;
+    float* grad = nullptr;
+    __nv_bfloat16* wbf = nullptr;
+    int step = 0;
+    int cap = 0;  // batch capacity of the training scratch
+    int act = 0;  // 0 ReLU, 1 identity
+    float *H1 = nullptr, *H2 = nullptr, *D1 = nullptr, *D2 = nullptr, *DY = nullptr, *Y = nullptr, *L = nullptr;
+    MlpWeights weights() const { return MlpWeights{wbf, theta, act}; }
+};
+
+__global__ void sum_in_order_kernel(const float* v, int n, float scale, float* out) {
+    __shared__ double sh[CUTCELL_WARPS + 1];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += v[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) *out = (float)(s * scale);
+}
+
 struct cutcell_ctx {
     int kind = KIND_CSR;
     int n = 0;
@@ -116,6 +139,11 @@ struct cutcell_ctx {
     unsigned* bar = nullptr;  // control words, one 128-byte line each: [0] arrival, [32] err, [64] tile work, [96] cut work, [128..] debug
     DevResult* res = nullptr;
     int max_blocks = 0;
+    // learned preconditioner
+    cutcell_mlp* mlp = nullptr;
+    PatchMap pmap = {0, nullptr, nullptr, nullptr};
+    double* zl = nullptr;
+    double* rold = nullptr;
     // refinement
     double inner_tol = 1e-4;
     int inner_maxiter = 100000;
@@ -202,6 +230,24 @@ static int run_ir(cutcell_ctx* c, const OpHi& hi, const OpLo& lo, size_t smem, S
 }
 
 template <class Op>
+static int run_fcg(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, cudaStream_t s, int* blocks) {
+    auto kern = fcg_kernel<Op>;
+    const size_t op_al = (op_smem + 15) & ~(size_t)15;
+    const size_t smem = op_al + MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 3 * 64) * sizeof(float);
+    int st = ensure_part(c, kern, smem, blocks);
+    if (st) return st;
+    a.gs = make_gs(c, *blocks);
+    a.B = make_bufs(c);
+    LearnedArgs L;
+    L.W = c->mlp->weights();
+    L.pm = c->pmap;
+    L.z = c->zl;
+    L.rold = c->rold;
+    L.use_mlp = c->pmap.binv ? 2 : 1;
+    return launch_coop(kern, *blocks, smem, s, op, a, L, op_al);
+}
+
+template <class Op>
 static int run_apply(cutcell_ctx* c, const Op& op, size_t smem, const double* x, double* y, cudaStream_t s) {
     auto kern = apply_kernel<Op>;
     int blocks = 0;
@@ -224,6 +270,7 @@ static int tiles_run(cutcell_ctx* c, int mode, int precision, SolveArgs* a, cons
     TileOp<float, P1> o32{c->td, c->cut32};
     TileOp<__nv_bfloat16, P1> o16{c->td, c->cut16};
     const size_t sm = TileOp<double, P1>::smem_bytes();
+    if (mode == 2) return run_fcg(c, o64, sm, *a, s, blocks);
     if (mode == 1) {
         if (precision == CUTCELL_FP64) return run_apply(c, o64, sm, x, y, s);
         if (precision == CUTCELL_FP32_IR) return run_apply(c, o32, sm, x, y, s);
@@ -398,10 +445,12 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
                       int32_t precond, CutcellReport* report, void* stream) {
     if (!c || !b || !x || maxiter < 0 || !(tol >= 0.0)) return CUTCELL_E_ARG;
     if (precision < CUTCELL_FP64 || precision > CUTCELL_BF16_IR) return CUTCELL_E_ARG;
-    if (precond != CUTCELL_PRECOND_NONE && precond != CUTCELL_PRECOND_JACOBI) return CUTCELL_E_ARG;
+    if (precond < CUTCELL_PRECOND_NONE || precond > CUTCELL_PRECOND_JACOBI_LEARNED) return CUTCELL_E_ARG;
+    if (precond == CUTCELL_PRECOND_JACOBI_LEARNED && (!c->mlp || precision != CUTCELL_FP64 || c->kind != KIND_TILES))
+        return CUTCELL_E_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaSetDevice(c->device));
-    c->use_jacobi = (precond == CUTCELL_PRECOND_JACOBI);
+    c->use_jacobi = (precond != CUTCELL_PRECOND_NONE);
     SolveArgs a;
     memset(&a, 0, sizeof(a));
     a.b = b;
@@ -425,6 +474,8 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
             st = run_ir(c, c->csr64, c->csr32, 0, a, s, &blocks);
         else
             st = run_ir(c, c->csr64, c->csr16, 0, a, s, &blocks);
+    } else if (precond == CUTCELL_PRECOND_JACOBI_LEARNED) {
+        st = tiles_dispatch(c, 2, precision, &a, nullptr, nullptr, s, &blocks);
     } else {
         st = tiles_dispatch(c, 0, precision, &a, nullptr, nullptr, s, &blocks);
     }
@@ -487,13 +538,133 @@ int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
-    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->yfv, c->psmall, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
                     c->p,     c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     delete c;
+    return CUTCELL_OK;
+}
+
+int cutcell_mlp_create(const float* theta_init, int32_t activation, cutcell_mlp** out) {
+    if (!theta_init || !out || activation < 0 || activation > 1) return CUTCELL_E_ARG;
+    cutcell_mlp* m = new cutcell_mlp();
+    m->act = activation;
+    CK(cudaGetDevice(&m->device));
+    CK(cudaMalloc(&m->theta, MLP_NPARAM * sizeof(float)));
+    CK(cudaMalloc(&m->m, MLP_NPARAM * sizeof(float)));
+    CK(cudaMalloc(&m->v, MLP_NPARAM * sizeof(float)));
+    CK(cudaMalloc(&m->grad, MLP_NPARAM * sizeof(float)));
+    CK(cudaMalloc(&m->wbf, MLP_NW * sizeof(__nv_bfloat16)));
+    CK(cudaMemcpy(m->theta, theta_init, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToDevice));
+    CK(cudaMemset(m->m, 0, MLP_NPARAM * sizeof(float)));
+    CK(cudaMemset(m->v, 0, MLP_NPARAM * sizeof(float)));
+    mlp_refresh_bf16_kernel<<<ceil_div(MLP_NPARAM, 256), 256>>>(m->theta, m->wbf);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    *out = m;
+    return CUTCELL_OK;
+}
+
+int cutcell_mlp_params(cutcell_mlp* m, float* theta_out, float* grad_out) {
+    if (!m) return CUTCELL_E_ARG;
+    if (theta_out) CK(cudaMemcpy(theta_out, m->theta, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToDevice));
+    if (grad_out) CK(cudaMemcpy(grad_out, m->grad, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToDevice));
+    return CUTCELL_OK;
+}
+
+int cutcell_mlp_forward(cutcell_mlp* m, const float* X, int32_t batch, float* Y, void* stream) {
+    if (!m || !X || !Y || batch < 0) return CUTCELL_E_ARG;
+    if (batch == 0) return CUTCELL_OK;
+    const size_t smem = MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 3 * 64) * sizeof(float);
+    CK(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mlp_forward_kernel<<<ceil_div(batch, CUTCELL_WARPS), CUTCELL_BLOCK, smem, (cudaStream_t)stream>>>(m->weights(), X,
+                                                                                                   batch, Y);
+    CK(cudaGetLastError());
+    return CUTCELL_OK;
+}
+
+int cutcell_mlp_train_step(cutcell_mlp* m, const float* X, const float* T, int32_t batch, float lr, float* loss_out,
+                           void* stream) {
+    if (!m || !X || !T || batch <= 0) return CUTCELL_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (batch > m->cap) {
+        float** bufs[] = {&m->H1, &m->H2, &m->D1, &m->D2, &m->DY, &m->Y};
+        for (float** b : bufs) {
+            if (*b) cudaFree(*b);
+            CK(cudaMalloc(b, (size_t)batch * 64 * sizeof(float)));
+        }
+        if (m->L) cudaFree(m->L);
+        CK(cudaMalloc(&m->L, (size_t)batch * sizeof(float)));
+        m->cap = batch;
+    }
+    const size_t smem = MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 6 * 64) * sizeof(float);
+    CK(cudaFuncSetAttribute(mlp_fwd_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int nblk = ceil_div(batch, CUTCELL_WARPS) < 4 * 148 ? ceil_div(batch, CUTCELL_WARPS) : 4 * 148;
+    mlp_fwd_bwd_kernel<<<nblk, CUTCELL_BLOCK, smem, s>>>(m->weights(), X, T, batch, m->H1, m->H2, m->D1, m->D2, m->DY,
+                                                        m->Y, m->L);
+    mlp_grad_kernel<<<ceil_div(MLP_NPARAM, 128), 128, 0, s>>>(X, m->H1, m->H2, m->D1, m->D2, m->DY, batch, m->grad);
+    if (loss_out) sum_in_order_kernel<<<1, CUTCELL_BLOCK, 0, s>>>(m->L, batch, 1.0f / (float)((long)batch * 64), loss_out);
+    if (lr > 0.f) {
+        m->step += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - powf(b1, (float)m->step), c2 = 1.f - powf(b2, (float)m->step);
+        mlp_adam_kernel<<<ceil_div(MLP_NPARAM, 256), 256, 0, s>>>(m->theta, m->m, m->v, m->grad, m->wbf, lr, b1, b2,
+                                                                  1e-8f, c1, c2);
+    }
+    CK(cudaGetLastError());
+    return CUTCELL_OK;
+}
+
+int cutcell_mlp_destroy(cutcell_mlp* m) {
+    if (!m) return CUTCELL_E_ARG;
+    cudaDeviceSynchronize();
+    void* bufs[] = {m->theta, m->m, m->v, m->grad, m->wbf, m->H1, m->H2, m->D1, m->D2, m->DY, m->Y, m->L};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    delete m;
+    return CUTCELL_OK;
+}
+
+int cutcell_patch_features(cutcell_ctx* c, const int32_t* patch_red, const float* patch_gamma, int32_t n_patch,
+                           const double* r, float* X, float* S, void* stream) {
+    if (!c || !patch_red || !patch_gamma || !r || !X || !S || n_patch < 0) return CUTCELL_E_ARG;
+    if (n_patch == 0) return CUTCELL_OK;
+    PatchMap pm{n_patch, patch_red, patch_gamma, nullptr};
+    patch_features_kernel<<<ceil_div(n_patch, CUTCELL_WARPS), CUTCELL_BLOCK, 0, (cudaStream_t)stream>>>(pm, r, c->dinv,
+                                                                                                      X, S);
+    CK(cudaGetLastError());
+    return CUTCELL_OK;
+}
+
+int cutcell_patch_targets(cutcell_ctx* c, const int32_t* patch_red, int32_t n_patch, const double* e,
+                          const double* r, const float* S, float* T, void* stream) {
+    if (!c || !patch_red || !e || !r || !S || !T || n_patch < 0) return CUTCELL_E_ARG;
+    if (n_patch == 0) return CUTCELL_OK;
+    PatchMap pm{n_patch, patch_red, nullptr, nullptr};
+    patch_targets_kernel<<<ceil_div((long)n_patch * 64, 256), 256, 0, (cudaStream_t)stream>>>(pm, e, r, c->dinv, S, T);
+    CK(cudaGetLastError());
+    return CUTCELL_OK;
+}
+
+int cutcell_pcg_set_block_inverses(cutcell_ctx* c, const double* binv) {
+    if (!c || c->kind != KIND_TILES || !c->mlp) return CUTCELL_E_ARG;
+    c->pmap.binv = binv;
+    return CUTCELL_OK;
+}
+
+int cutcell_pcg_set_learned(cutcell_ctx* c, cutcell_mlp* m, const int32_t* patch_red, const float* patch_gamma,
+                            int32_t n_patch) {
+    if (!c || c->kind != KIND_TILES) return CUTCELL_E_ARG;
+    if (m && (!patch_red || !patch_gamma || n_patch <= 0)) return CUTCELL_E_ARG;
+    c->mlp = m;
+    c->pmap = PatchMap{n_patch, patch_red, patch_gamma, nullptr};
+    if (m && !c->zl) {
+        CK(cudaMalloc(&c->zl, (size_t)c->n * sizeof(double)));
+        CK(cudaMalloc(&c->rold, (size_t)c->n * sizeof(double)));
+    }
     return CUTCELL_OK;
 }
 

@@ -1,0 +1,535 @@
+// Learned preconditioner: a patch-wise MLP (128 -> 64 -> 64 -> 64, ReLU) with
+// BF16 weights and FP32 accumulation, its training kernels (forward /
+// backward / Adam), and the flexible PCG that applies it after Jacobi.
+//
+// Features of one 4x4x4 DOF patch: u = D^{-1} r on the patch's 64 DOFs,
+// s = ||u|| + 1e-300, input x = [u / s, gamma * u / s] (gamma = fluid-mass
+// ratio of each DOF, 0 off the fluid).  The correction is
+// z = D^{-1} r + s * (y(x) - y(-x)) / 2.
+// Every reduced DOF belongs to exactly one patch, so z is written once.
+#pragma once
+
+#include "ops.cuh"
+
+#define MLP_IN 128
+#define MLP_H 64
+#define MLP_OUT 64
+#define MLP_PATCH 64
+// FP32 parameter vector layout: W1[128][64], b1[64], W2[64][64], b2[64], W3[64][64], b3[64]
+#define MLP_OFF_W1 0
+#define MLP_OFF_B1 (MLP_IN * MLP_H)
+#define MLP_OFF_W2 (MLP_OFF_B1 + MLP_H)
+#define MLP_OFF_B2 (MLP_OFF_W2 + MLP_H * MLP_H)
+#define MLP_OFF_W3 (MLP_OFF_B2 + MLP_H)
+#define MLP_OFF_B3 (MLP_OFF_W3 + MLP_H * MLP_OUT)
+#define MLP_NPARAM (MLP_OFF_B3 + MLP_OUT)
+#define MLP_NW (MLP_IN * MLP_H + MLP_H * MLP_H + MLP_H * MLP_OUT)  // weights only
+
+struct MlpWeights {
+    const __nv_bfloat16* w;  // BF16 weights W1|W2|W3 (row-major [in][out])
+    const float* theta;      // FP32 parameters (biases read from here)
+    int act;                 // hidden activation: 0 ReLU, 1 identity (a linear network)
+};
+
+__device__ __forceinline__ float mlp_act(float v, int act) { return act ? v : fmaxf(v, 0.f); }
+__device__ __forceinline__ float mlp_dact(float z, int act) { return act ? 1.f : (z > 0.f ? 1.f : 0.f); }
+
+// Shared-memory image of the network: BF16 weights + FP32 biases.
+struct MlpSmem {
+    __nv_bfloat16* w;  // MLP_NW
+    float* b;          // 3 * 64
+    int act;
+    __host__ __device__ static constexpr size_t bytes() { return MLP_NW * sizeof(__nv_bfloat16) + 3 * 64 * sizeof(float); }
+};
+
+__device__ __forceinline__ MlpSmem mlp_load_smem(const MlpWeights& W, char* base) {
+    MlpSmem s;
+    s.w = reinterpret_cast<__nv_bfloat16*>(base);
+    s.b = reinterpret_cast<float*>(base + MLP_NW * sizeof(__nv_bfloat16));
+    s.act = W.act;
+    for (int k = threadIdx.x; k < MLP_NW; k += blockDim.x) s.w[k] = W.w[k];
+    for (int k = threadIdx.x; k < 64; k += blockDim.x) {
+        s.b[k] = W.theta[MLP_OFF_B1 + k];
+        s.b[64 + k] = W.theta[MLP_OFF_B2 + k];
+        s.b[128 + k] = W.theta[MLP_OFF_B3 + k];
+    }
+    return s;
+}
+
+// One sample per warp. x (128 floats) and h (2 x 64 floats) are the warp's
+// shared scratch; on return y[0..63] (in h2 storage) holds the output, and
+// z1/z2 (pre-activations) are written when non-null.  Lane l owns outputs l
+// and l + 32 of every layer.
+__device__ __forceinline__ void mlp_forward_warp(const MlpSmem& S, const float* x, float* h1, float* h2, float* y,
+                                                 float* z1, float* z2) {
+    const int l = threadIdx.x & 31;
+    const __nv_bfloat16* W1 = S.w;
+    const __nv_bfloat16* W2 = S.w + MLP_IN * MLP_H;
+    const __nv_bfloat16* W3 = W2 + MLP_H * MLP_H;
+    float a0 = S.b[l], a1 = S.b[l + 32];
+#pragma unroll 8
+    for (int i = 0; i < MLP_IN; ++i) {
+        const float xi = x[i];
+        a0 = fmaf(xi, __bfloat162float(W1[i * MLP_H + l]), a0);
+        a1 = fmaf(xi, __bfloat162float(W1[i * MLP_H + l + 32]), a1);
+    }
+    if (z1) {
+        z1[l] = a0;
+        z1[l + 32] = a1;
+    }
+    h1[l] = mlp_act(a0, S.act);
+    h1[l + 32] = mlp_act(a1, S.act);
+    __syncwarp();
+    a0 = S.b[64 + l];
+    a1 = S.b[64 + l + 32];
+#pragma unroll 8
+    for (int i = 0; i < MLP_H; ++i) {
+        const float hi = h1[i];
+        a0 = fmaf(hi, __bfloat162float(W2[i * MLP_H + l]), a0);
+        a1 = fmaf(hi, __bfloat162float(W2[i * MLP_H + l + 32]), a1);
+    }
+    if (z2) {
+        z2[l] = a0;
+        z2[l + 32] = a1;
+    }
+    h2[l] = mlp_act(a0, S.act);
+    h2[l + 32] = mlp_act(a1, S.act);
+    __syncwarp();
+    a0 = S.b[128 + l];
+    a1 = S.b[128 + l + 32];
+#pragma unroll 8
+    for (int i = 0; i < MLP_H; ++i) {
+        const float hi = h2[i];
+        a0 = fmaf(hi, __bfloat162float(W3[i * MLP_OUT + l]), a0);
+        a1 = fmaf(hi, __bfloat162float(W3[i * MLP_OUT + l + 32]), a1);
+    }
+    __syncwarp();
+    y[l] = a0;
+    y[l + 32] = a1;
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Training kernels (batch of samples, row-major [batch][features]).
+// ---------------------------------------------------------------------------
+
+// forward + per-sample backward: stores z1, z2, h1, h2 and the deltas
+// dz1, dz2, dy for the weight-gradient kernel; loss partial per sample.
+__global__ void __launch_bounds__(256) mlp_fwd_bwd_kernel(MlpWeights W, const float* X, const float* Tgt, int batch,
+                                                          float* H1, float* H2, float* D1, float* D2, float* DY,
+                                                          float* Y, float* sample_loss) {
+    extern __shared__ __align__(16) char smem[];
+    MlpSmem S = mlp_load_smem(W, smem);
+    float* scratch = reinterpret_cast<float*>(smem + MlpSmem::bytes());
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+    float* xs = scratch + warp * (MLP_IN + 6 * 64);
+    float* h1 = xs + MLP_IN;
+    float* h2 = h1 + 64;
+    float* y = h2 + 64;
+    float* z1 = y + 64;
+    float* z2 = z1 + 64;
+    float* d = z2 + 64;
+    const __nv_bfloat16* W2 = S.w + MLP_IN * MLP_H;
+    const __nv_bfloat16* W3 = W2 + MLP_H * MLP_H;
+    const float scale = 2.0f / (float)((long)batch * MLP_OUT);
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
+    for (int b = gw; b < batch; b += nw) {
+        for (int i = l; i < MLP_IN; i += 32) xs[i] = X[(size_t)b * MLP_IN + i];
+        __syncwarp();
+        mlp_forward_warp(S, xs, h1, h2, y, z1, z2);
+        // dy = 2 (y - t) / (batch * n_out)
+        float loss = 0.f;
+        for (int o = l; o < MLP_OUT; o += 32) {
+            const float e = y[o] - Tgt[(size_t)b * MLP_OUT + o];
+            loss += e * e;
+            d[o] = scale * e;
+            DY[(size_t)b * MLP_OUT + o] = scale * e;
+            Y[(size_t)b * MLP_OUT + o] = y[o];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+        if (l == 0) sample_loss[b] = loss;
+        __syncwarp();
+        // dz2 = (dy W3^T) * (z2 > 0)
+        float g0 = 0.f, g1 = 0.f;
+        for (int o = 0; o < MLP_OUT; ++o) {
+            const float dyo = d[o];
+            g0 = fmaf(dyo, __bfloat162float(W3[l * MLP_OUT + o]), g0);
+            g1 = fmaf(dyo, __bfloat162float(W3[(l + 32) * MLP_OUT + o]), g1);
+        }
+        g0 *= mlp_dact(z2[l], S.act);
+        g1 *= mlp_dact(z2[l + 32], S.act);
+        __syncwarp();
+        d[l] = g0;
+        d[l + 32] = g1;
+        D2[(size_t)b * 64 + l] = g0;
+        D2[(size_t)b * 64 + l + 32] = g1;
+        H2[(size_t)b * 64 + l] = h2[l];
+        H2[(size_t)b * 64 + l + 32] = h2[l + 32];
+        __syncwarp();
+        // dz1 = (dz2 W2^T) * (z1 > 0)
+        g0 = 0.f;
+        g1 = 0.f;
+        for (int o = 0; o < MLP_H; ++o) {
+            const float v = d[o];
+            g0 = fmaf(v, __bfloat162float(W2[l * MLP_H + o]), g0);
+            g1 = fmaf(v, __bfloat162float(W2[(l + 32) * MLP_H + o]), g1);
+        }
+        g0 *= mlp_dact(z1[l], S.act);
+        g1 *= mlp_dact(z1[l + 32], S.act);
+        D1[(size_t)b * 64 + l] = g0;
+        D1[(size_t)b * 64 + l + 32] = g1;
+        H1[(size_t)b * 64 + l] = h1[l];
+        H1[(size_t)b * 64 + l + 32] = h1[l + 32];
+        __syncwarp();
+    }
+}
+
+// Parameter gradients, one thread per parameter, samples summed in order.
+__global__ void mlp_grad_kernel(const float* X, const float* H1, const float* H2, const float* D1, const float* D2,
+                                const float* DY, int batch, float* grad) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= MLP_NPARAM) return;
+    const float* A;
+    const float* G;
+    int lda, ldg, i, o;
+    if (k < MLP_OFF_B1) {
+        i = k / MLP_H; o = k % MLP_H; A = X; lda = MLP_IN; G = D1; ldg = 64;
+    } else if (k < MLP_OFF_W2) {
+        i = -1; o = k - MLP_OFF_B1; A = nullptr; lda = 0; G = D1; ldg = 64;
+    } else if (k < MLP_OFF_B2) {
+        i = (k - MLP_OFF_W2) / MLP_H; o = (k - MLP_OFF_W2) % MLP_H; A = H1; lda = 64; G = D2; ldg = 64;
+    } else if (k < MLP_OFF_W3) {
+        i = -1; o = k - MLP_OFF_B2; A = nullptr; lda = 0; G = D2; ldg = 64;
+    } else if (k < MLP_OFF_B3) {
+        i = (k - MLP_OFF_W3) / MLP_OUT; o = (k - MLP_OFF_W3) % MLP_OUT; A = H2; lda = 64; G = DY; ldg = 64;
+    } else {
+        i = -1; o = k - MLP_OFF_B3; A = nullptr; lda = 0; G = DY; ldg = 64;
+    }
+    float s = 0.f;
+    if (A) {
+        for (int b = 0; b < batch; ++b) s = fmaf(A[(size_t)b * lda + i], G[(size_t)b * ldg + o], s);
+    } else {
+        for (int b = 0; b < batch; ++b) s += G[(size_t)b * ldg + o];
+    }
+    grad[k] = s;
+}
+
+// Adam step on the FP32 parameters and refresh of the BF16 weights.
+__global__ void mlp_adam_kernel(float* theta, float* m, float* v, const float* grad, __nv_bfloat16* wbf, float lr,
+                                float b1, float b2, float eps, float c1, float c2) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= MLP_NPARAM) return;
+    const float g = grad[k];
+    const float mk = b1 * m[k] + (1.f - b1) * g;
+    const float vk = b2 * v[k] + (1.f - b2) * g * g;
+    m[k] = mk;
+    v[k] = vk;
+    const float p = theta[k] - lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+    theta[k] = p;
+    // W1 | b1 | W2 | b2 | W3 | b3  ->  W1 | W2 | W3 in the BF16 image
+    int w = -1;
+    if (k < MLP_OFF_B1) w = k;
+    else if (k >= MLP_OFF_W2 && k < MLP_OFF_B2) w = MLP_IN * MLP_H + (k - MLP_OFF_W2);
+    else if (k >= MLP_OFF_W3 && k < MLP_OFF_B3) w = MLP_IN * MLP_H + MLP_H * MLP_H + (k - MLP_OFF_W3);
+    if (w >= 0) wbf[w] = __float2bfloat16(p);
+}
+
+__global__ void mlp_refresh_bf16_kernel(const float* theta, __nv_bfloat16* wbf) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= MLP_NPARAM) return;
+    int w = -1;
+    if (k < MLP_OFF_B1) w = k;
+    else if (k >= MLP_OFF_W2 && k < MLP_OFF_B2) w = MLP_IN * MLP_H + (k - MLP_OFF_W2);
+    else if (k >= MLP_OFF_W3 && k < MLP_OFF_B3) w = MLP_IN * MLP_H + MLP_H * MLP_H + (k - MLP_OFF_W3);
+    if (w >= 0) wbf[w] = __float2bfloat16(theta[k]);
+}
+
+// Inference over a batch (warp per sample).
+__global__ void __launch_bounds__(256) mlp_forward_kernel(MlpWeights W, const float* X, int batch, float* Y) {
+    extern __shared__ __align__(16) char smem[];
+    MlpSmem S = mlp_load_smem(W, smem);
+    float* scratch = reinterpret_cast<float*>(smem + MlpSmem::bytes());
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+    float* xs = scratch + warp * (MLP_IN + 3 * 64);
+    float* h1 = xs + MLP_IN;
+    float* h2 = h1 + 64;
+    float* y = h2 + 64;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
+    for (int b = gw; b < batch; b += nw) {
+        for (int i = l; i < MLP_IN; i += 32) xs[i] = X[(size_t)b * MLP_IN + i];
+        __syncwarp();
+        mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
+        Y[(size_t)b * MLP_OUT + l] = y[l];
+        Y[(size_t)b * MLP_OUT + l + 32] = y[l + 32];
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Patch features from a reduced residual (dataset generation and tests).
+// X[k] = [u/s, gamma], S[k] = s with u = dinv * r on the patch.
+// ---------------------------------------------------------------------------
+struct PatchMap {
+    int n_patch;
+    const int* red;      // [n_patch][64] reduced index or -1
+    const float* gamma;  // [n_patch][64]
+    const double* binv;  // optional [n_patch][64][64] exact patch inverses (block Jacobi)
+};
+
+__device__ __forceinline__ float patch_features_warp(const PatchMap& pm, int k, const double* r, const double* dinv,
+                                                     float* x) {
+    const int l = threadIdx.x & 31;
+    double u0 = 0.0, u1 = 0.0;
+    const int j0 = __ldg(pm.red + (size_t)k * 64 + l), j1 = __ldg(pm.red + (size_t)k * 64 + l + 32);
+    if (j0 >= 0) u0 = __ldg(dinv + j0) * __ldcg(r + j0);
+    if (j1 >= 0) u1 = __ldg(dinv + j1) * __ldcg(r + j1);
+    double ss = u0 * u0 + u1 * u1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    const double s = sqrt(ss) + 1e-300;
+    x[l] = (float)(u0 / s);
+    x[l + 32] = (float)(u1 / s);
+    x[64 + l] = __ldg(pm.gamma + (size_t)k * 64 + l) * (float)(u0 / s);
+    x[64 + l + 32] = __ldg(pm.gamma + (size_t)k * 64 + l + 32) * (float)(u1 / s);
+    __syncwarp();
+    return (float)s;
+}
+
+__global__ void patch_features_kernel(PatchMap pm, const double* r, const double* dinv, float* X, float* Sc) {
+    __shared__ float xs[8][MLP_IN];
+    const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
+    for (int k = gw; k < pm.n_patch; k += nw) {
+        const float s = patch_features_warp(pm, k, r, dinv, xs[warp]);
+        for (int i = l; i < MLP_IN; i += 32) X[(size_t)k * MLP_IN + i] = xs[warp][i];
+        if (l == 0) Sc[k] = s;
+        __syncwarp();
+    }
+}
+
+// Training targets: T[k][q] = (e_j - dinv_j r_j) / s_k on the patch DOFs.
+__global__ void patch_targets_kernel(PatchMap pm, const double* e, const double* r, const double* dinv, const float* Sc,
+                                     float* T) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < pm.n_patch * 64; t += gridDim.x * blockDim.x) {
+        const int k = t >> 6;
+        const int j = __ldg(pm.red + t);
+        float v = 0.f;
+        if (j >= 0) v = (float)((e[j] - dinv[j] * r[j]) / (double)Sc[k]);
+        T[t] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Flexible PCG with z = D^{-1} r + s * mlp(x) (Polak-Ribiere beta).
+// Safeguard: if r.z_mlp <= 0.1 * r.D^{-1}r the iteration uses Jacobi.
+// ---------------------------------------------------------------------------
+struct LearnedArgs {
+    MlpWeights W;
+    PatchMap pm;
+    double* z;      // [n] learned correction target
+    double* rold;   // [n]
+    int use_mlp;
+};
+
+__device__ __forceinline__ void learned_precond_phase(const LearnedArgs& L, const PcgBufs& B, const MlpSmem& S,
+                                                      float* scratch) {
+    const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
+    float* xs = scratch + warp * (MLP_IN + 3 * 64);
+    float* h1 = xs + MLP_IN;
+    float* h2 = h1 + 64;
+    float* y = h2 + 64;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
+    if (L.use_mlp == 2) {  // exact block Jacobi on the patches (reference ceiling)
+        for (int k = gw; k < L.pm.n_patch; k += nw) {
+            double rp0 = 0.0, rp1 = 0.0;
+            const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
+            if (j0 >= 0) rp0 = __ldcg(B.r + j0);
+            if (j1 >= 0) rp1 = __ldcg(B.r + j1);
+            double z0 = 0.0, z1 = 0.0;
+            const double* Bk = L.pm.binv + (size_t)k * 4096;
+            for (int q = 0; q < 64; ++q) {
+                const double rq = __shfl_sync(0xffffffffu, q < 32 ? rp0 : rp1, q & 31);
+                z0 += __ldg(Bk + l * 64 + q) * rq;
+                z1 += __ldg(Bk + (l + 32) * 64 + q) * rq;
+            }
+            if (j0 >= 0) L.z[j0] = z0;
+            if (j1 >= 0) L.z[j1] = z1;
+        }
+        return;
+    }
+    // odd part of the network in the residual: y = (f(u, g) - f(-u, g)) / 2,
+    // so the correction is linear under sign changes of r like the patch
+    // inverse it approximates
+    for (int k = gw; k < L.pm.n_patch; k += nw) {
+        const float s = patch_features_warp(L.pm, k, B.r, B.dinv, xs);
+        mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
+        const float yp0 = y[l], yp1 = y[l + 32];
+        __syncwarp();
+        xs[l] = -xs[l];
+        xs[l + 32] = -xs[l + 32];
+        xs[64 + l] = -xs[64 + l];
+        xs[64 + l + 32] = -xs[64 + l + 32];
+        __syncwarp();
+        mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
+        const float ya = 0.5f * (yp0 - y[l]), yb = 0.5f * (yp1 - y[l + 32]);
+        const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
+        if (j0 >= 0) L.z[j0] = B.dinv[j0] * __ldcg(B.r + j0) + (double)s * (double)ya;
+        if (j1 >= 0) L.z[j1] = B.dinv[j1] * __ldcg(B.r + j1) + (double)s * (double)yb;
+        __syncwarp();
+    }
+}
+
+template <class Op>
+__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) fcg_kernel(Op op, SolveArgs a, LearnedArgs L, size_t op_smem) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double sh[CUTCELL_WARPS + 1];
+    char* smem_mlp = reinterpret_cast<char*>(sm) + op_smem;
+    float* scratch = reinterpret_cast<float*>(smem_mlp + MlpSmem::bytes());
+    const PcgBufs& B = a.B;
+    const int n = B.n, nb = gridDim.x;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    double* part = B.part;
+    const GridSync& gs = a.gs;
+    // network image loaded once; the operator's shared memory precedes it
+    MlpSmem S;
+    if (L.use_mlp == 1) S = mlp_load_smem(L.W, smem_mlp);
+    // x = 0, r = b, z = M(r)
+    double bb = 0.0;
+    for (int i = gtid; i < n; i += gstride) {
+        a.x[i] = 0.0;
+        B.r[i] = a.b[i];
+        bb += a.b[i] * a.b[i];
+    }
+    bb = block_sum(bb, sh);
+    if (threadIdx.x == 0) part[1 * nb + blockIdx.x] = bb;
+    int status = CUTCELL_E_NOCONV, k = 0;
+    double rel = 1.0;
+    if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
+    double bnorm = sqrt(grid_reduce(part + 1 * nb, nb, sh));
+    if (bnorm == 0.0) bnorm = 1.0;
+    if (L.use_mlp) learned_precond_phase(L, B, S, scratch);
+    if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
+    double rz = 0.0, rzj = 0.0;
+    for (int i = gtid; i < n; i += gstride) {
+        const double ri = B.r[i], zj = B.dinv[i] * ri;
+        const double zi = L.use_mlp ? __ldcg(L.z + i) : zj;
+        rz += ri * zi;
+        rzj += ri * zj;
+    }
+    rz = block_sum(rz, sh);
+    rzj = block_sum(rzj, sh);
+    if (threadIdx.x == 0) {
+        part[0 * nb + blockIdx.x] = rz;
+        part[6 * nb + blockIdx.x] = rzj;
+    }
+    if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
+    rz = grid_reduce(part + 0 * nb, nb, sh);
+    rzj = grid_reduce(part + 6 * nb, nb, sh);
+    bool jac = !L.use_mlp || !(rz > 0.1 * rzj);
+    if (jac) rz = rzj;
+    for (int i = gtid; i < n; i += gstride) B.p[i] = jac ? B.dinv[i] * B.r[i] : __ldcg(L.z + i);
+    if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
+    for (k = 1; k <= a.maxiter && status != CUTCELL_E_BARRIER; ++k) {
+        double pap = op.apply(B.p, B.Ap, gs, sm);
+        if (grid_error(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        pap = block_sum(pap, sh);
+        if (threadIdx.x == 0) part[2 * nb + blockIdx.x] = pap;
+        if (!grid_sync(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        pap = grid_reduce(part + 2 * nb, nb, sh);
+        if (!(pap > 0.0) || !isfinite(pap)) {
+            status = CUTCELL_E_BREAKDOWN;
+            break;
+        }
+        const double alpha = rz / pap;
+        double rr = 0.0;
+        for (int i = gtid; i < n; i += gstride) {
+            a.x[i] += alpha * B.p[i];
+            const double ro = B.r[i];
+            L.rold[i] = ro;
+            const double ri = ro - alpha * __ldcg(B.Ap + i);
+            B.r[i] = ri;
+            rr += ri * ri;
+        }
+        rr = block_sum(rr, sh);
+        if (threadIdx.x == 0) part[3 * nb + blockIdx.x] = rr;
+        if (!grid_sync(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        rel = sqrt(grid_reduce(part + 3 * nb, nb, sh)) / bnorm;
+        if (!isfinite(rel)) {
+            status = CUTCELL_E_NAN;
+            break;
+        }
+        if (rel <= a.tol) {
+            status = CUTCELL_OK;
+            break;
+        }
+        if (L.use_mlp) learned_precond_phase(L, B, S, scratch);
+        if (!grid_sync(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        // rz_new = r.z, rzo = r_old.z (Polak-Ribiere), Jacobi versions for the safeguard
+        double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
+        for (int i = gtid; i < n; i += gstride) {
+            const double ri = B.r[i], ro = L.rold[i], zj = B.dinv[i] * ri;
+            const double zi = L.use_mlp ? __ldcg(L.z + i) : zj;
+            d0 += ri * zi;
+            d1 += ro * zi;
+            d2 += ri * zj;
+            d3 += ro * zj;
+        }
+        d0 = block_sum(d0, sh);
+        d1 = block_sum(d1, sh);
+        d2 = block_sum(d2, sh);
+        d3 = block_sum(d3, sh);
+        if (threadIdx.x == 0) {
+            part[4 * nb + blockIdx.x] = d0;
+            part[5 * nb + blockIdx.x] = d1;
+            part[6 * nb + blockIdx.x] = d2;
+            part[7 * nb + blockIdx.x] = d3;
+        }
+        if (!grid_sync(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        d0 = grid_reduce(part + 4 * nb, nb, sh);
+        d1 = grid_reduce(part + 5 * nb, nb, sh);
+        d2 = grid_reduce(part + 6 * nb, nb, sh);
+        d3 = grid_reduce(part + 7 * nb, nb, sh);
+        jac = !L.use_mlp || !(d0 > 0.1 * d2);
+        const double rzn = jac ? d2 : d0;
+        const double beta = (rzn - (jac ? d3 : d1)) / rz;
+        rz = rzn;
+        for (int i = gtid; i < n; i += gstride) {
+            const double zi = jac ? B.dinv[i] * B.r[i] : __ldcg(L.z + i);
+            B.p[i] = zi + beta * B.p[i];
+        }
+        if (!grid_sync(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+    }
+    const int iters = k > a.maxiter ? a.maxiter : k;
+    double true_rel = -1.0;
+    if (status != CUTCELL_E_BARRIER && !grid_error(gs))
+        true_rel = true_residual(op, B, a.b, a.x, bnorm, gs, sm, sh, nullptr);
+    if (grid_error(gs)) status = CUTCELL_E_BARRIER;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.res->status = status;
+        a.res->iterations = iters;
+        a.res->outer = 1;
+        a.res->rel = rel;
+        a.res->true_rel = true_rel;
+    }
+}

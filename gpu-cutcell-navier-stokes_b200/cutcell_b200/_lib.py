@@ -31,6 +31,8 @@ PRECISIONS = {"fp64": FP64, "fp32-ir": FP32_IR, "bf16-ir": BF16_IR}
 PRECOND_NONE = 0
 PRECOND_JACOBI = 1
 PRECOND_JACOBI_LEARNED = 2
+MLP_NPARAM = 16576
+MLP_IN, MLP_H, MLP_OUT = 128, 64, 64
 
 
 class CutcellLibraryError(RuntimeError):
@@ -108,6 +110,15 @@ SIGNATURES = {
     "cutcell_ext_gather": (C.c_int, [_P, _P, _P, _P]),
     "cutcell_ext_scatter": (C.c_int, [_P, _P, _P, _P]),
     "cutcell_destroy": (C.c_int, [_P]),
+    "cutcell_mlp_create": (C.c_int, [_P, C.c_int32, C.POINTER(_P)]),
+    "cutcell_mlp_params": (C.c_int, [_P, _P, _P]),
+    "cutcell_mlp_forward": (C.c_int, [_P, _P, C.c_int32, _P, _P]),
+    "cutcell_mlp_train_step": (C.c_int, [_P, _P, _P, C.c_int32, C.c_float, _P, _P]),
+    "cutcell_mlp_destroy": (C.c_int, [_P]),
+    "cutcell_patch_features": (C.c_int, [_P, _P, _P, C.c_int32, _P, _P, _P, _P]),
+    "cutcell_patch_targets": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P, _P, _P]),
+    "cutcell_pcg_set_learned": (C.c_int, [_P, _P, _P, _P, C.c_int32]),
+    "cutcell_pcg_set_block_inverses": (C.c_int, [_P, _P]),
     "cutcell_status_string": (C.c_char_p, [C.c_int]),
     "cutcell_last_error": (C.c_char_p, []),
 }

@@ -296,7 +296,9 @@ class CutCellOperator:
         if x is None:
             x = torch.empty_like(b)
         rep = _lib.CutcellReport()
-        pc = {"none": _lib.PRECOND_NONE, "jacobi": _lib.PRECOND_JACOBI}[preconditioner]
+        pc = {"none": _lib.PRECOND_NONE, "jacobi": _lib.PRECOND_JACOBI, "jacobi+learned": _lib.PRECOND_JACOBI_LEARNED}[
+            preconditioner
+        ]
         _lib.check(
             self._lib.cutcell_pcg_solve(
                 self._ctx, b.data_ptr(), x.data_ptr(), float(tol), int(maxiter), _lib.PRECISIONS[precision], pc,

@@ -119,7 +119,9 @@ int cutcell_set_refinement(cutcell_ctx* ctx, double inner_tol, int32_t inner_max
  * solve_gpu_cg (code/fast_solver_backends.py:236-274), run as one persistent
  * cooperative launch with no host round trip per iteration. precision is
  * CUTCELL_FP64 (plain) or an iterative-refinement form; precond is
- * CUTCELL_PRECOND_NONE or CUTCELL_PRECOND_JACOBI.  Blocks until done. */
+ * CUTCELL_PRECOND_NONE, CUTCELL_PRECOND_JACOBI, or
+ * CUTCELL_PRECOND_JACOBI_LEARNED (flexible PCG, FP64, needs
+ * cutcell_pcg_set_learned).  Blocks until done. */
 int cutcell_pcg_solve(cutcell_ctx* ctx, const double* b, double* x, double tol, int32_t maxiter,
                       int32_t precision, int32_t precond, CutcellReport* report, void* stream);
 
@@ -131,6 +133,40 @@ int cutcell_apply(cutcell_ctx* ctx, const double* x, double* y, int32_t precisio
  * code/bell_3d_core.py:471-542); uses the tile descriptor's E arrays. */
 int cutcell_ext_gather(cutcell_ctx* ctx, const double* x_red, double* x_full, void* stream);
 int cutcell_ext_scatter(cutcell_ctx* ctx, const double* y_full, double* y_red, void* stream);
+
+/* ---- learned preconditioner (no counterpart in the reference: an addition
+ * of this build; its solve is flexible PCG with z = D^{-1} r + s * mlp(x) on
+ * 4x4x4 DOF patches, u = D^{-1} r, x = [u / s, gamma * u / s] (128 features),
+ * s = patch norm, odd part (mlp(x) - mlp(-x)) / 2,
+ * MLP 128 -> 64 -> 64 -> 64 (ReLU), BF16 weights, FP32 accumulation) ---- */
+typedef struct cutcell_mlp cutcell_mlp;
+#define CUTCELL_MLP_NPARAM 16576  /* FP32: W1[128][64] b1[64] W2[64][64] b2[64] W3[64][64] b3[64] */
+/* activation of the two hidden layers: 0 = ReLU, 1 = identity (linear network) */
+int cutcell_mlp_create(const float* theta_init, int32_t activation, cutcell_mlp** out);
+/* copies of the FP32 parameters and of the last gradient (either may be NULL) */
+int cutcell_mlp_params(cutcell_mlp* mlp, float* theta_out, float* grad_out);
+/* Y[batch][64] = mlp(X[batch][128]) */
+int cutcell_mlp_forward(cutcell_mlp* mlp, const float* X, int32_t batch, float* Y, void* stream);
+/* loss = mean((mlp(X) - T)^2); gradients of it; an Adam step when lr > 0;
+ * loss_out (device float, may be NULL) */
+int cutcell_mlp_train_step(cutcell_mlp* mlp, const float* X, const float* T, int32_t batch, float lr, float* loss_out,
+                           void* stream);
+int cutcell_mlp_destroy(cutcell_mlp* mlp);
+/* features X[n_patch][128] and scales S[n_patch] of a reduced residual r
+ * (patch_red[n_patch][64]: reduced index or -1; patch_gamma: fluid ratios) */
+int cutcell_patch_features(cutcell_ctx* ctx, const int32_t* patch_red, const float* patch_gamma, int32_t n_patch,
+                           const double* r, float* X, float* S, void* stream);
+/* training targets T[n_patch][64] = (e - D^{-1} r) / S on the patch DOFs */
+int cutcell_patch_targets(cutcell_ctx* ctx, const int32_t* patch_red, int32_t n_patch, const double* e,
+                          const double* r, const float* S, float* T, void* stream);
+/* attach (mlp != NULL) or detach the learned correction used by
+ * CUTCELL_PRECOND_JACOBI_LEARNED (FP64, matrix-free contexts) */
+int cutcell_pcg_set_learned(cutcell_ctx* ctx, cutcell_mlp* mlp, const int32_t* patch_red, const float* patch_gamma,
+                            int32_t n_patch);
+
+/* replace the network by exact patch inverses binv[n_patch][64][64] (block
+ * Jacobi, the ceiling the network is trained towards); NULL restores the network */
+int cutcell_pcg_set_block_inverses(cutcell_ctx* ctx, const double* binv);
 
 int cutcell_destroy(cutcell_ctx* ctx);
 const char* cutcell_status_string(int status);
