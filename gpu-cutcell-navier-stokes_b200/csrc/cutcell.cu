@@ -1,11 +1,14 @@
 // C ABI of libcutcell_b200.so: contexts, cooperative launches, status codes.
 // The persistent kernels live in pcg.cuh / ops.cuh.
+#include <cmath>
 #include <cstdio>
+#include <vector>
 #include <cstring>
 #include <string>
 
 #include "pcg.cuh"
 #include "learned.cuh"
+#include "fastdiag.cuh"
 
 namespace {
 
@@ -106,6 +109,13 @@ __global__ void sum_in_order_kernel(const float* v, int n, float scale, float* o
     s = block_sum(s, sh);
     if (threadIdx.x == 0) *out = (float)(s * scale);
 }
+
+struct cutcell_fastdiag {
+    int device = 0;
+    FastDiagDev d;
+    double *X = nullptr, *T = nullptr, *UT = nullptr, *G = nullptr, *U = nullptr, *S2 = nullptr;
+    double *QxT = nullptr, *QyT = nullptr, *cosT = nullptr, *sinT = nullptr;
+};
 
 struct cutcell_ctx {
     int kind = KIND_CSR;
@@ -665,6 +675,124 @@ int cutcell_pcg_set_learned(cutcell_ctx* c, cutcell_mlp* m, const int32_t* patch
         CK(cudaMalloc(&c->zl, (size_t)c->n * sizeof(double)));
         CK(cudaMalloc(&c->rold, (size_t)c->n * sizeof(double)));
     }
+    return CUTCELL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// periodic-hill fast diagonalisation
+// ---------------------------------------------------------------------------
+
+__global__ void fd_transpose_kernel(int n, const double* A, double* AT) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < (long)n * n; t += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / n), j = (int)(t % n);
+        AT[(size_t)j * n + i] = A[t];
+    }
+}
+
+int cutcell_fastdiag_create(int32_t nr, int32_t nz, const double* M2, const double* Qx2, const double* Qy2,
+                            const double* mu, const double* kap, const double* Ainv, const double* Sinv,
+                            cutcell_fastdiag** out) {
+    if (!out || nr <= 0 || nz <= 0 || !M2 || !Qx2 || !Qy2 || !mu || !kap || !Ainv || !Sinv) return CUTCELL_E_ARG;
+    if ((size_t)6 * nr * sizeof(double) > 200 * 1024) return CUTCELL_E_SHAPE;  // per-mode vectors staged in shared memory
+    cutcell_fastdiag* f = new cutcell_fastdiag();
+    CK(cudaGetDevice(&f->device));
+    const size_t vec = (size_t)nz * nr * sizeof(double);
+    CK(cudaMalloc(&f->X, 6 * vec));
+    CK(cudaMalloc(&f->T, 6 * vec));
+    CK(cudaMalloc(&f->UT, 6 * vec));
+    CK(cudaMalloc(&f->G, 6 * vec));
+    CK(cudaMalloc(&f->U, 6 * vec));
+    CK(cudaMalloc(&f->S2, 2 * vec * 8));  // Gx Gy Gz DIV P Hx Hy Hz
+    CK(cudaMalloc(&f->QxT, (size_t)nr * nr * sizeof(double)));
+    CK(cudaMalloc(&f->QyT, (size_t)nr * nr * sizeof(double)));
+    CK(cudaMalloc(&f->cosT, (size_t)nz * nz * sizeof(double)));
+    CK(cudaMalloc(&f->sinT, (size_t)nz * nz * sizeof(double)));
+    std::vector<double> ct((size_t)nz * nz), st((size_t)nz * nz);
+    for (int a = 0; a < nz; ++a)
+        for (int b = 0; b < nz; ++b) {
+            // reduce a*b mod nz first so the angle stays in [0, 2 pi)
+            const double ang = 2.0 * M_PI * (double)((a * b) % nz) / nz;
+            ct[(size_t)a * nz + b] = std::cos(ang);
+            st[(size_t)a * nz + b] = std::sin(ang);
+        }
+    CK(cudaMemcpy(f->cosT, ct.data(), ct.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(f->sinT, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
+    fd_transpose_kernel<<<ceil_div((long)nr * nr, 256), 256>>>(nr, Qx2, f->QxT);
+    fd_transpose_kernel<<<ceil_div((long)nr * nr, 256), 256>>>(nr, Qy2, f->QyT);
+    FastDiagDev& d = f->d;
+    d.nr = nr;
+    d.nz = nz;
+    d.M2 = M2;
+    d.Qx2 = Qx2;
+    d.Qy2 = Qy2;
+    d.Qx2T = f->QxT;
+    d.Qy2T = f->QyT;
+    d.mu = mu;
+    d.kap = kap;
+    d.Ainv = Ainv;
+    d.Sinv = Sinv;
+    d.cosT = f->cosT;
+    d.sinT = f->sinT;
+    const int smem6 = (int)(6 * nr * sizeof(double)), smem2 = (int)(2 * nr * sizeof(double));
+    CK(cudaFuncSetAttribute(fd_mode_mv_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem6));
+    CK(cudaFuncSetAttribute(fd_mode_mv_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2));
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    *out = f;
+    return CUTCELL_OK;
+}
+
+static void fd_gemm(cudaStream_t s, int nr, const double* A, const double* X, VecSel sx, double* Y, VecSel sy,
+                    int nvec) {
+    dim3 grid(ceil_div(nr, FD_TR), ceil_div(nvec, FD_TV));
+    fd_shared_gemm_kernel<<<grid, 256, 0, s>>>(nr, A, X, sx, Y, sy, nvec);
+}
+
+int cutcell_fastdiag_solve(cutcell_fastdiag* f, const double* ux, const double* uy, const double* uz, double* ox,
+                           double* oy, double* oz, void* stream) {
+    if (!f || !ux || !uy || !uz || !ox || !oy || !oz) return CUTCELL_E_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const FastDiagDev& d = f->d;
+    const int nr = d.nr, nz = d.nz;
+    const size_t v2 = (size_t)2 * nz * nr;
+    double* Gx = f->S2;
+    double* Gy = Gx + v2;
+    double* Gz = Gy + v2;
+    double* DIV = Gz + v2;
+    double* P = DIV + v2;
+    double* Hx = P + v2;
+    double* Hy = Hx + v2;
+    double* Hz = Hy + v2;
+    const int ew = ceil_div((long)nz * nr * 3, 256);
+    const int rows = nr >= 1024 ? 64 : 16;
+    dim3 mv_grid(ceil_div(nr, rows), nz);
+    fd_dft_kernel<<<ew, 256, 0, s>>>(d, ux, uy, uz, f->X);
+    fd_gemm(s, nr, d.M2, f->X, VecSel{6, 0, 6}, f->T, VecSel{6, 0, 6}, 6 * nz);
+    fd_scale_mu_kernel<<<ceil_div((long)nz * 6 * nr, 256), 256, 0, s>>>(d, f->T);
+    fd_mode_mv_kernel<6><<<mv_grid, 256, 6 * nr * sizeof(double), s>>>(nr, d.Ainv, f->T, f->UT, nullptr, rows);
+    fd_gemm(s, nr, d.Qx2, f->UT, VecSel{2, 0, 6}, Gx, VecSel{2, 0, 2}, 2 * nz);
+    fd_gemm(s, nr, d.Qy2, f->UT, VecSel{2, 2, 6}, Gy, VecSel{2, 0, 2}, 2 * nz);
+    fd_gemm(s, nr, d.M2, f->UT, VecSel{2, 4, 6}, Gz, VecSel{2, 0, 2}, 2 * nz);
+    fd_div_kernel<<<ceil_div((long)nz * nr, 256), 256, 0, s>>>(d, Gx, Gy, Gz, DIV);
+    fd_mode_mv_kernel<2><<<mv_grid, 256, 2 * nr * sizeof(double), s>>>(nr, d.Sinv, DIV, P, nullptr, rows);
+    fd_gemm(s, nr, d.Qx2T, P, VecSel{2, 0, 2}, Hx, VecSel{2, 0, 2}, 2 * nz);
+    fd_gemm(s, nr, d.Qy2T, P, VecSel{2, 0, 2}, Hy, VecSel{2, 0, 2}, 2 * nz);
+    fd_gemm(s, nr, d.M2, P, VecSel{2, 0, 2}, Hz, VecSel{2, 0, 2}, 2 * nz);
+    fd_grad_kernel<<<ceil_div((long)nz * nr, 256), 256, 0, s>>>(d, Hx, Hy, Hz, f->G);
+    fd_mode_mv_kernel<6><<<mv_grid, 256, 6 * nr * sizeof(double), s>>>(nr, d.Ainv, f->G, f->U, f->UT, rows);
+    fd_idft_kernel<<<ew, 256, 0, s>>>(d, f->U, ox, oy, oz);
+    CK(cudaGetLastError());
+    return CUTCELL_OK;
+}
+
+int cutcell_fastdiag_destroy(cutcell_fastdiag* f) {
+    if (!f) return CUTCELL_E_ARG;
+    cudaSetDevice(f->device);
+    cudaDeviceSynchronize();
+    void* bufs[] = {f->X, f->T, f->UT, f->G, f->U, f->S2, f->QxT, f->QyT, f->cosT, f->sinT};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    delete f;
     return CUTCELL_OK;
 }
 

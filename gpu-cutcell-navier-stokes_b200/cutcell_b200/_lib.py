@@ -119,6 +119,9 @@ SIGNATURES = {
     "cutcell_patch_targets": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P, _P, _P]),
     "cutcell_pcg_set_learned": (C.c_int, [_P, _P, _P, _P, C.c_int32]),
     "cutcell_pcg_set_block_inverses": (C.c_int, [_P, _P]),
+    "cutcell_fastdiag_create": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    "cutcell_fastdiag_solve": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
+    "cutcell_fastdiag_destroy": (C.c_int, [_P]),
     "cutcell_status_string": (C.c_char_p, [C.c_int]),
     "cutcell_last_error": (C.c_char_p, []),
 }

@@ -168,6 +168,20 @@ int cutcell_pcg_set_learned(cutcell_ctx* ctx, cutcell_mlp* mlp, const int32_t* p
  * Jacobi, the ceiling the network is trained towards); NULL restores the network */
 int cutcell_pcg_set_block_inverses(cutcell_ctx* ctx, const double* binv);
 
+/* ---- periodic-hill fast diagonalisation (FastDiagHill, cpp/include/cut/hill_fastdiag.h:20-80) ----
+ * create: the reduced 2D forms M2, Qx2, Qy2 (nr x nr, row-major), the z
+ * symbols mu, kap (nz), and the per-mode inverses Ainv[nz][nr][nr],
+ * Sinv[nz][nr][nr] that FastDiagHill::build (:26-43) forms; all device
+ * pointers, kept by reference.  solve: FastDiagHill::solve (:47-79) on FieldH
+ * arrays (v[m*nz + iz]); asynchronous on `stream`. */
+typedef struct cutcell_fastdiag cutcell_fastdiag;
+int cutcell_fastdiag_create(int32_t nr, int32_t nz, const double* M2, const double* Qx2, const double* Qy2,
+                            const double* mu, const double* kap, const double* Ainv, const double* Sinv,
+                            cutcell_fastdiag** out);
+int cutcell_fastdiag_solve(cutcell_fastdiag* fd, const double* ux, const double* uy, const double* uz, double* ox,
+                           double* oy, double* oz, void* stream);
+int cutcell_fastdiag_destroy(cutcell_fastdiag* fd);
+
 int cutcell_destroy(cutcell_ctx* ctx);
 const char* cutcell_status_string(int status);
 /* Last CUDA error text seen by the library (diagnostics). */
