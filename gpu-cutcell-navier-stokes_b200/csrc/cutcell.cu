@@ -115,6 +115,7 @@ struct cutcell_fastdiag {
     FastDiagDev d;
     double *X = nullptr, *T = nullptr, *UT = nullptr, *G = nullptr, *U = nullptr, *S2 = nullptr;
     double *QxT = nullptr, *QyT = nullptr, *cosT = nullptr, *sinT = nullptr;
+    double* part = nullptr;
 };
 
 struct cutcell_ctx {
@@ -703,6 +704,7 @@ int cutcell_fastdiag_create(int32_t nr, int32_t nz, const double* M2, const doub
     CK(cudaMalloc(&f->G, 6 * vec));
     CK(cudaMalloc(&f->U, 6 * vec));
     CK(cudaMalloc(&f->S2, 2 * vec * 8));  // Gx Gy Gz DIV P Hx Hy Hz
+    CK(cudaMalloc(&f->part, (size_t)FD_KSPLIT * 6 * vec));  // split-K partial products
     CK(cudaMalloc(&f->QxT, (size_t)nr * nr * sizeof(double)));
     CK(cudaMalloc(&f->QyT, (size_t)nr * nr * sizeof(double)));
     CK(cudaMalloc(&f->cosT, (size_t)nz * nz * sizeof(double)));
@@ -743,9 +745,10 @@ int cutcell_fastdiag_create(int32_t nr, int32_t nz, const double* M2, const doub
 }
 
 static void fd_gemm(cudaStream_t s, int nr, const double* A, const double* X, VecSel sx, double* Y, VecSel sy,
-                    int nvec) {
-    dim3 grid(ceil_div(nr, FD_TR), ceil_div(nvec, FD_TV));
-    fd_shared_gemm_kernel<<<grid, 256, 0, s>>>(nr, A, X, sx, Y, sy, nvec);
+                    int nvec, double* part) {
+    dim3 grid(ceil_div(nr, FD_TR), ceil_div(nvec, FD_TV), FD_KSPLIT);
+    fd_shared_gemm_kernel<<<grid, FD_GEMM_THREADS, 0, s>>>(nr, A, X, sx, part, nvec);
+    fd_sum_ksplit_kernel<<<ceil_div((long)nvec * nr, 256), 256, 0, s>>>(nr, nvec, FD_KSPLIT, part, Y, sy);
 }
 
 int cutcell_fastdiag_solve(cutcell_fastdiag* f, const double* ux, const double* uy, const double* uz, double* ox,
@@ -764,22 +767,22 @@ int cutcell_fastdiag_solve(cutcell_fastdiag* f, const double* ux, const double* 
     double* Hy = Hx + v2;
     double* Hz = Hy + v2;
     const int ew = ceil_div((long)nz * nr * 3, 256);
-    const int rows = nr >= 1024 ? 64 : 16;
+    const int rows = nr >= 1024 ? 128 : 32;
     dim3 mv_grid(ceil_div(nr, rows), nz);
     fd_dft_kernel<<<ew, 256, 0, s>>>(d, ux, uy, uz, f->X);
-    fd_gemm(s, nr, d.M2, f->X, VecSel{6, 0, 6}, f->T, VecSel{6, 0, 6}, 6 * nz);
+    fd_gemm(s, nr, d.M2, f->X, VecSel{6, 0, 6}, f->T, VecSel{6, 0, 6}, 6 * nz, f->part);
     fd_scale_mu_kernel<<<ceil_div((long)nz * 6 * nr, 256), 256, 0, s>>>(d, f->T);
-    fd_mode_mv_kernel<6><<<mv_grid, 256, 6 * nr * sizeof(double), s>>>(nr, d.Ainv, f->T, f->UT, nullptr, rows);
-    fd_gemm(s, nr, d.Qx2, f->UT, VecSel{2, 0, 6}, Gx, VecSel{2, 0, 2}, 2 * nz);
-    fd_gemm(s, nr, d.Qy2, f->UT, VecSel{2, 2, 6}, Gy, VecSel{2, 0, 2}, 2 * nz);
-    fd_gemm(s, nr, d.M2, f->UT, VecSel{2, 4, 6}, Gz, VecSel{2, 0, 2}, 2 * nz);
+    fd_mode_mv_kernel<6><<<mv_grid, FD_MV_THREADS, 6 * nr * sizeof(double), s>>>(nr, d.Ainv, f->T, f->UT, nullptr, rows);
+    fd_gemm(s, nr, d.Qx2, f->UT, VecSel{2, 0, 6}, Gx, VecSel{2, 0, 2}, 2 * nz, f->part);
+    fd_gemm(s, nr, d.Qy2, f->UT, VecSel{2, 2, 6}, Gy, VecSel{2, 0, 2}, 2 * nz, f->part);
+    fd_gemm(s, nr, d.M2, f->UT, VecSel{2, 4, 6}, Gz, VecSel{2, 0, 2}, 2 * nz, f->part);
     fd_div_kernel<<<ceil_div((long)nz * nr, 256), 256, 0, s>>>(d, Gx, Gy, Gz, DIV);
-    fd_mode_mv_kernel<2><<<mv_grid, 256, 2 * nr * sizeof(double), s>>>(nr, d.Sinv, DIV, P, nullptr, rows);
-    fd_gemm(s, nr, d.Qx2T, P, VecSel{2, 0, 2}, Hx, VecSel{2, 0, 2}, 2 * nz);
-    fd_gemm(s, nr, d.Qy2T, P, VecSel{2, 0, 2}, Hy, VecSel{2, 0, 2}, 2 * nz);
-    fd_gemm(s, nr, d.M2, P, VecSel{2, 0, 2}, Hz, VecSel{2, 0, 2}, 2 * nz);
+    fd_mode_mv_kernel<2><<<mv_grid, FD_MV_THREADS, 2 * nr * sizeof(double), s>>>(nr, d.Sinv, DIV, P, nullptr, rows);
+    fd_gemm(s, nr, d.Qx2T, P, VecSel{2, 0, 2}, Hx, VecSel{2, 0, 2}, 2 * nz, f->part);
+    fd_gemm(s, nr, d.Qy2T, P, VecSel{2, 0, 2}, Hy, VecSel{2, 0, 2}, 2 * nz, f->part);
+    fd_gemm(s, nr, d.M2, P, VecSel{2, 0, 2}, Hz, VecSel{2, 0, 2}, 2 * nz, f->part);
     fd_grad_kernel<<<ceil_div((long)nz * nr, 256), 256, 0, s>>>(d, Hx, Hy, Hz, f->G);
-    fd_mode_mv_kernel<6><<<mv_grid, 256, 6 * nr * sizeof(double), s>>>(nr, d.Ainv, f->G, f->U, f->UT, rows);
+    fd_mode_mv_kernel<6><<<mv_grid, FD_MV_THREADS, 6 * nr * sizeof(double), s>>>(nr, d.Ainv, f->G, f->U, f->UT, rows);
     fd_idft_kernel<<<ew, 256, 0, s>>>(d, f->U, ox, oy, oz);
     CK(cudaGetLastError());
     return CUTCELL_OK;
@@ -789,7 +792,7 @@ int cutcell_fastdiag_destroy(cutcell_fastdiag* f) {
     if (!f) return CUTCELL_E_ARG;
     cudaSetDevice(f->device);
     cudaDeviceSynchronize();
-    void* bufs[] = {f->X, f->T, f->UT, f->G, f->U, f->S2, f->QxT, f->QyT, f->cosT, f->sinT};
+    void* bufs[] = {f->X, f->T, f->UT, f->G, f->U, f->S2, f->QxT, f->QyT, f->cosT, f->sinT, f->part};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete f;

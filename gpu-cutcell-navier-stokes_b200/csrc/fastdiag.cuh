@@ -86,52 +86,88 @@ __device__ __forceinline__ size_t vec_off(const VecSel& s, int v, int nr) {
 }
 
 #define FD_TR 64
-#define FD_TV 16
-#define FD_TK 32
-__global__ void __launch_bounds__(256) fd_shared_gemm_kernel(int nr, const double* A, const double* X, VecSel sx,
-                                                            double* Y, VecSel sy, int nvec) {
-    __shared__ double As[FD_TR][FD_TK + 1];
-    __shared__ double Xs[FD_TV][FD_TK + 1];
+#define FD_TV 64
+#define FD_TK 16
+#define FD_GEMM_THREADS 256
+#define FD_KSPLIT 4
+// 256 threads as 16 x 16, each owning a 4-row x 4-vector register tile of the
+// 64 x 64 block tile.  blockIdx.z takes one of FD_KSPLIT slices of the inner
+// dimension and writes its partial product to slice z of Ypart (vector v of
+// slice z at Ypart + (z * nvec + v) * nr); fd_sum_ksplit_kernel adds the
+// slices in order (deterministic, no atomics).
+__global__ void __launch_bounds__(FD_GEMM_THREADS) fd_shared_gemm_kernel(int nr, const double* A, const double* X,
+                                                                        VecSel sx, double* Ypart, int nvec) {
+    __shared__ double As[FD_TK][FD_TR + 2];
+    __shared__ double Xs[FD_TK][FD_TV + 2];
     const int r0 = blockIdx.x * FD_TR, v0 = blockIdx.y * FD_TV;
-    const int tr = threadIdx.x % 16, tv = threadIdx.x / 16;  // 16 x 16 threads, 4 rows x 1 vector each
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int j0 = 0; j0 < nr; j0 += FD_TK) {
+    const int kchunk = (nr + gridDim.z - 1) / gridDim.z;
+    const int kb = blockIdx.z * kchunk, ke = min(nr, kb + kchunk);
+    const int tr = threadIdx.x % 16, tv = threadIdx.x / 16;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int j0 = kb; j0 < ke; j0 += FD_TK) {
         for (int e = threadIdx.x; e < FD_TR * FD_TK; e += blockDim.x) {
             const int rr = e / FD_TK, jj = e % FD_TK;
             const int r = r0 + rr, j = j0 + jj;
-            As[rr][jj] = (r < nr && j < nr) ? A[(size_t)r * nr + j] : 0.0;
+            As[jj][rr] = (r < nr && j < ke) ? A[(size_t)r * nr + j] : 0.0;
         }
         for (int e = threadIdx.x; e < FD_TV * FD_TK; e += blockDim.x) {
             const int vv = e / FD_TK, jj = e % FD_TK;
             const int v = v0 + vv, j = j0 + jj;
-            Xs[vv][jj] = (v < nvec && j < nr) ? X[vec_off(sx, v, nr) + j] : 0.0;
+            Xs[jj][vv] = (v < nvec && j < ke) ? X[vec_off(sx, v, nr) + j] : 0.0;
         }
         __syncthreads();
-#pragma unroll 8
-        for (int jj = 0; jj < FD_TK; ++jj) {
-            const double xv = Xs[tv][jj];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] += As[tr + 16 * q][jj] * xv;
+        for (int jj = 0; jj < FD_TK; ++jj) {
+            double a[4], x[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                a[q] = As[jj][tr + 16 * q];
+                x[q] = Xs[jj][tv + 16 * q];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int w = 0; w < 4; ++w) acc[q][w] += a[q] * x[w];
         }
         __syncthreads();
     }
-    const int v = v0 + tv;
-    if (v < nvec) {
-        const size_t off = vec_off(sy, v, nr);
+    double* Yz = Ypart + (size_t)blockIdx.z * nvec * nr;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        const int v = v0 + tv + 16 * w;
+        if (v >= nvec) continue;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int r = r0 + tr + 16 * q;
-            if (r < nr) Y[off + r] = acc[q];
+            if (r < nr) Yz[(size_t)v * nr + r] = acc[q][w];
         }
     }
 }
 
+// Y[sel(v)] = sum_z Ypart[z][v]  (slices added in order)
+__global__ void fd_sum_ksplit_kernel(int nr, int nvec, int ks, const double* Ypart, double* Y, VecSel sy) {
+    const long total = (long)nvec * nr;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const int v = (int)(t / nr), r = (int)(t % nr);
+        double s = 0.0;
+        for (int z = 0; z < ks; ++z) s += Ypart[(size_t)z * total + t];
+        Y[vec_off(sy, v, nr) + r] = s;
+    }
+}
+
 // Per-mode dense matvec with NV right-hand sides, streaming B_k once:
-// Y_k[v] = alpha * B_k X_k[v] (+ Ysub_k[v] when sub != 0, i.e. Y = Ysub - B X).
-// grid (row chunks, modes); X_k staged in shared memory; one warp per row.
+// Y_k[v] = B_k X_k[v], or Y_k[v] = Ysub_k[v] - B_k X_k[v] when Ysub != 0.
+// grid (row chunks, modes); X_k staged in shared memory; each warp streams
+// 4 rows at a time (4 independent loads per column step) for memory-level
+// parallelism.
+#define FD_MV_THREADS 512
 template <int NV>
-__global__ void __launch_bounds__(256) fd_mode_mv_kernel(int nr, const double* B, const double* X, double* Y,
-                                                        const double* Ysub, int rows_per_block) {
+__global__ void __launch_bounds__(FD_MV_THREADS) fd_mode_mv_kernel(int nr, const double* B, const double* X, double* Y,
+                                                                  const double* Ysub, int rows_per_block) {
     extern __shared__ double xs[];  // NV * nr
     const int k = blockIdx.y;
     const double* Xk = X + (size_t)k * NV * nr;
@@ -141,24 +177,40 @@ __global__ void __launch_bounds__(256) fd_mode_mv_kernel(int nr, const double* B
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int r_begin = blockIdx.x * rows_per_block;
     const int r_end = min(nr, r_begin + rows_per_block);
-    for (int r = r_begin + warp; r < r_end; r += nw) {
-        double acc[NV];
+    for (int r = r_begin + 4 * warp; r < r_end; r += 4 * nw) {
+        double acc[4][NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) acc[v] = 0.0;
-        const double* row = Bk + (size_t)r * nr;
-#pragma unroll 4
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) acc[q][v] = 0.0;
+        const double* row[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) row[q] = Bk + (size_t)min(r + q, nr - 1) * nr;
+#pragma unroll 2
         for (int j = lane; j < nr; j += 32) {
-            const double b = __ldg(row + j);
+            double b[4];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) acc[v] += b * xs[v * nr + j];
-        }
-#pragma unroll
-        for (int v = 0; v < NV; ++v) acc[v] = warp_sum(acc[v]);
-        if (lane == 0) {
+            for (int q = 0; q < 4; ++q) b[q] = __ldg(row[q] + j);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                const size_t o = ((size_t)k * NV + v) * nr + r;
-                Y[o] = Ysub ? Ysub[o] - acc[v] : acc[v];
+                const double xv = xs[v * nr + j];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q][v] += b[q] * xv;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) acc[q][v] = warp_sum(acc[q][v]);
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (r + q >= r_end) continue;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    const size_t o = ((size_t)k * NV + v) * nr + r + q;
+                    Y[o] = Ysub ? Ysub[o] - acc[q][v] : acc[q][v];
+                }
             }
         }
     }
