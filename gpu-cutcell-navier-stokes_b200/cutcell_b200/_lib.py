@@ -122,6 +122,11 @@ SIGNATURES = {
     "cutcell_fastdiag_create": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "cutcell_fastdiag_solve": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
     "cutcell_fastdiag_destroy": (C.c_int, [_P]),
+    "cutcell_pcg_solve_csr_noalloc": (
+        C.c_int,
+        [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, C.c_double, C.c_int32, C.c_int32, C.POINTER(CutcellReport), _P],
+    ),
+    "cutcell_noalloc_last_error": (C.c_char_p, []),
     "cutcell_status_string": (C.c_char_p, [C.c_int]),
     "cutcell_last_error": (C.c_char_p, []),
 }

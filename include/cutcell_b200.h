@@ -182,6 +182,24 @@ int cutcell_fastdiag_solve(cutcell_fastdiag* fd, const double* ux, const double*
                            double* oy, double* oz, void* stream);
 int cutcell_fastdiag_destroy(cutcell_fastdiag* fd);
 
+/* Allocation-free Jacobi-PCG on a device CSR matrix.  No counterpart in the
+ * reference: it serves callers that cannot allocate device memory when they
+ * solve (a framework's caching allocator holding the device, loops that must
+ * not take the synchronisation of cudaMalloc/cudaFree, fixed memory budgets).
+ * Same algorithm, arguments and report as cutcell_pcg_create_csr +
+ * cutcell_pcg_solve (FP64, precond NONE or JACOBI), but every working array
+ * lives in one fixed file-scope device array of the library, sized for
+ * n <= 65536 unknowns and <= 1024 persistent blocks (about 2.2 MB per GPU,
+ * held until the process exits).  Larger n returns CUTCELL_E_SHAPE.  The
+ * first call on each device resolves the array's address and the grid size;
+ * make that first call before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * report->elapsed_ms is 0 (no events are created on this path). */
+int cutcell_pcg_solve_csr_noalloc(int32_t n, int32_t nnz, const int32_t* indptr, const int32_t* indices,
+                                  const double* data, const double* b, double* x, double tol, int32_t maxiter,
+                                  int32_t precond, CutcellReport* report, void* stream);
+const char* cutcell_noalloc_last_error(void);
+
 int cutcell_destroy(cutcell_ctx* ctx);
 const char* cutcell_status_string(int status);
 /* Last CUDA error text seen by the library (diagnostics). */
