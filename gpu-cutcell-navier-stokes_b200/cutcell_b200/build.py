@@ -35,11 +35,18 @@ def build_setup(force: bool = False) -> Path:
     hdr = ROOT.parent / "include" / "cutcell_setup.h"
     if out.exists() and not force and all(out.stat().st_mtime >= d.stat().st_mtime for d in (src, hdr)):
         return out
-    cxx = os.environ.get("CXX", "g++")
-    cmd = [cxx, "-std=c++17", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", str(src), "-o", str(out) + ".tmp"]
-    subprocess.run(cmd, check=True, cwd=str(ROOT))
-    os.replace(str(out) + ".tmp", out)
-    return out
+    # $CXX first; a toolchain without libgomp (OpenMP) falls through to the next
+    cands = [c for c in (os.environ.get("CXX"), shutil.which("g++"), "/usr/bin/g++") if c]
+    last = None
+    for cxx in dict.fromkeys(cands):
+        cmd = [cxx, "-std=c++17", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", str(src), "-o",
+               str(out) + ".tmp"]
+        r = subprocess.run(cmd, cwd=str(ROOT), capture_output=True, text=True)
+        if r.returncode == 0:
+            os.replace(str(out) + ".tmp", out)
+            return out
+        last = f"{' '.join(cmd)}\n{r.stderr}"
+    raise RuntimeError(f"cannot build the setup library:\n{last}")
 
 
 def build(verbose: bool = False, force: bool = False) -> Path:
