@@ -326,6 +326,13 @@ const char* cutcell_status_string(int status) {
 }
 
 const char* cutcell_last_error(void) { return g_last_error.c_str(); }
+}
+
+// Library-internal (C++ linkage, not exported in the header): lets the other
+// translation units report through cutcell_last_error.
+void cutcell_internal_set_error(const std::string& what) { g_last_error = what; }
+
+extern "C" {
 
 int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const int32_t* indices, const double* data,
                            cutcell_ctx** out) {

@@ -97,6 +97,15 @@ class CutcellTileDesc(C.Structure):
     ]
 
 
+class CutcellBatchConfig(C.Structure):
+    _fields_ = [
+        ("cluster", C.c_int32),
+        ("threads", C.c_int32),
+        ("smem_matrix", C.c_int32),
+        ("teams", C.c_int32),
+    ]
+
+
 # name -> (restype, argtypes); every symbol declared in include/cutcell_b200.h
 SIGNATURES = {
     "cutcell_pcg_create_csr": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, C.POINTER(_P)]),
@@ -122,6 +131,11 @@ SIGNATURES = {
     "cutcell_fastdiag_create": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "cutcell_fastdiag_solve": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
     "cutcell_fastdiag_destroy": (C.c_int, [_P]),
+    "cutcell_batch_create": (C.c_int, [C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    "cutcell_batch_configure": (C.c_int, [_P, C.POINTER(CutcellBatchConfig), _P, _P]),
+    "cutcell_batch_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "cutcell_batch_solve": (C.c_int, [_P, _P, _P, C.c_double, C.c_int32, C.c_int32, _P, _P]),
+    "cutcell_batch_destroy": (C.c_int, [_P]),
     "cutcell_pcg_solve_csr_noalloc": (
         C.c_int,
         [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, C.c_double, C.c_int32, C.c_int32, C.POINTER(CutcellReport), _P],

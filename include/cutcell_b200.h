@@ -182,6 +182,49 @@ int cutcell_fastdiag_solve(cutcell_fastdiag* fd, const double* ux, const double*
                            double* oy, double* oz, void* stream);
 int cutcell_fastdiag_destroy(cutcell_fastdiag* fd);
 
+/* ---- batched persistent Jacobi-PCG over many uneven systems ----
+ * Replaces the one-system-at-a-time loop of the reference's solver sweeps
+ * (code/fast_solver_workbench.py:169-176 calling solve_cpu_cg / solve_gpu_cg,
+ * code/fast_solver_backends.py:90-132,194-289) with one persistent launch.
+ * Per system the iteration, stopping test and report are those of
+ * cutcell_pcg_solve (FP64, precond NONE or JACOBI).
+ *
+ * create: n[i], nnz[i] are HOST arrays (1 <= n[i] <= 16384); indptr, indices,
+ * data are DEVICE arrays holding the systems back to back: system i owns
+ * n[i] + 1 row offsets (values 0..nnz[i], relative to the system), nnz[i]
+ * column indices (0..n[i]-1, relative to the system) and nnz[i] values.  The
+ * caller keeps them alive while the context exists.
+ * configure: the launch shape and, per system (HOST arrays of n_problems),
+ * lanes_per_row (power of two <= 32) and the claim order (a permutation;
+ * teams take systems in this order, heaviest first).  A team is a cluster of
+ * `cluster` CTAs; up to smem_matrix bytes of shared memory per CTA hold the
+ * CTA's CSR slice when it fits (else it is read from global memory).
+ * solve: rhs / x are DEVICE arrays packed like the rows (system i at
+ * sum_{j<i} n[j]); reports is a HOST array of n_problems.  The solve is a
+ * captured CUDA graph (reset of the work counter, the persistent kernel, the
+ * copy of the per-system results), re-captured when the arguments or the
+ * configuration change; the call waits for it.  elapsed_ms is the device
+ * time of the whole batch; blocks is the cluster size.  Returns
+ * CUTCELL_E_SHAPE if a system's CSR arrays are malformed (that system's
+ * report has status CUTCELL_E_SHAPE), else CUTCELL_OK; per-system outcomes
+ * are in the reports. */
+typedef struct cutcell_batch cutcell_batch;
+typedef struct {
+    int32_t cluster;      /* CTAs per team: 1, 2, 4 or 8 */
+    int32_t threads;      /* threads per CTA: multiple of 32, <= 512 */
+    int32_t smem_matrix;  /* bytes per CTA for a staged CSR slice (multiple of 16; 0 = never stage) */
+    int32_t teams;        /* concurrent teams (0 = as many as fit, at most n_problems) */
+} CutcellBatchConfig;
+int cutcell_batch_create(int32_t n_problems, const int32_t* n, const int32_t* nnz, const int32_t* indptr,
+                         const int32_t* indices, const double* data, cutcell_batch** out);
+int cutcell_batch_configure(cutcell_batch* batch, const CutcellBatchConfig* cfg, const int32_t* lanes_per_row,
+                            const int32_t* order);
+/* teams launched and dynamic shared memory per CTA of the current configuration */
+int cutcell_batch_info(const cutcell_batch* batch, int32_t* teams, int32_t* smem_bytes);
+int cutcell_batch_solve(cutcell_batch* batch, const double* rhs, double* x, double tol, int32_t maxiter,
+                        int32_t precond, CutcellReport* reports, void* stream);
+int cutcell_batch_destroy(cutcell_batch* batch);
+
 /* Allocation-free Jacobi-PCG on a device CSR matrix.  No counterpart in the
  * reference: it serves callers that cannot allocate device memory when they
  * solve (a framework's caching allocator holding the device, loops that must
