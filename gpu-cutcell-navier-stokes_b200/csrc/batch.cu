@@ -10,9 +10,9 @@
 //     claim problems from a global counter in a host-chosen order (heaviest
 //     first), so uneven sizes balance without any grid-wide barrier.
 //   * A problem's rows are split into C contiguous slices, one per CTA.  Each
-//     CTA keeps x, r, A p and D^-1 of its rows, and a full copy of p, in
-//     shared memory; after each p update every CTA stores its slice of p into
-//     all C copies through distributed shared memory (DSMEM).
+//     CTA keeps x, r, A p and D^-1 of its rows, and full-length copies of z
+//     and p, in shared memory; after each r update every CTA stores its slice
+//     of z into all C copies of z through distributed shared memory (DSMEM).
 //   * A CTA's CSR slice is staged once per problem into shared memory (16-bit
 //     column indices) when it fits the configured budget; otherwise it is
 //     read from global memory (L2-resident for these sizes) every iteration.
@@ -20,7 +20,8 @@
 //     every CTA's slot array, one hardware cluster barrier, then every CTA adds
 //     the C partials in rank order -- all CTAs hold the same bits and take the
 //     same branches, so the cluster barriers are always matched.
-// Three cluster barriers per iteration (p published, p.Ap, r.r / r.z).
+// Two cluster barriers per iteration: p.Ap, and r.r / r.z together with the
+// gather of z = D^-1 r; every CTA then forms the whole p = z + beta p itself.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -52,7 +53,15 @@ struct BatchProblem {
 struct BatchResult {
     int status, iterations;
     double rel, true_rel;
+    unsigned long long t0, t1;  // %globaltimer (ns) when the team took / finished the system
+    int team, pad;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 struct BatchArgs {
     const BatchProblem* prob;
@@ -75,11 +84,12 @@ struct BatchArgs {
 
 // Dynamic shared-memory layout (byte offsets, each 16-byte aligned).
 struct BatchSmem {
-    int pfull, x, r, q, d, slots, mat, total;
+    int pfull, zfull, x, r, q, d, slots, mat, total;
     __host__ __device__ static int vec_bytes(int n) { return 8 * ((n + 1) & ~1); }
     __host__ __device__ BatchSmem(int n_max, int rows_max, int mat_bytes) {
         pfull = 0;
-        x = pfull + vec_bytes(n_max);
+        zfull = pfull + vec_bytes(n_max);
+        x = zfull + vec_bytes(n_max);
         r = x + vec_bytes(rows_max);
         q = r + vec_bytes(rows_max);
         d = q + vec_bytes(rows_max);
@@ -113,6 +123,8 @@ struct Team {
 };
 
 // Team-wide sums of NV per-thread values; every CTA ends with identical bits.
+// Warp partials -> warp 0 (fixed shuffle tree) -> lane c stores the CTA's
+// partial into rank c's slot -> one team barrier -> rank-ordered sum.
 template <int NV>
 __device__ __forceinline__ void team_sum(double (&v)[NV], double* sh, double* slots, int group, const Team& t) {
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -124,12 +136,12 @@ __device__ __forceinline__ void team_sum(double (&v)[NV], double* sh, double* sl
     }
     __syncthreads();
     double* gs = slots + group * 3 * BATCH_MAX_CLUSTER;
-    if (threadIdx.x == 0) {
+    if (w == 0) {
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
-            double s = 0.0;
-            for (int i = 0; i < nw; ++i) s += sh[q * 16 + i];
-            for (unsigned c = 0; c < t.C; ++c) *t.at(gs + q * BATCH_MAX_CLUSTER + t.rank, c) = s;
+            double s = (l < nw) ? sh[q * 16 + l] : 0.0;
+            s = warp_sum(s);
+            if (l < (int)t.C) *t.at(gs + q * BATCH_MAX_CLUSTER + t.rank, (unsigned)l) = s;
         }
     }
     t.sync();
@@ -144,6 +156,7 @@ __device__ __forceinline__ void team_sum(double (&v)[NV], double* sh, double* sl
 // q[i] = sum_k val[k] pin[col[k]] over the CTA's rows, tpr lanes per row; returns
 // this thread's share of sum_i pdot[i] q[i] (pdot may be null).  The row loop has
 // the same trip count on every lane, so the group shuffles are always full-warp.
+// Each lane keeps four independent accumulators so that its loads overlap.
 template <typename ColT, bool LDG>
 __device__ __forceinline__ double spmv_rows(int nown, int tl, const int* rp, int rp_base, const ColT* col,
                                             const double* val, const double* pin, double* qout,
@@ -154,16 +167,31 @@ __device__ __forceinline__ double spmv_rows(int nown, int tl, const int* rp, int
     double dot = 0.0;
     for (int base = 0; base < nown; base += groups) {
         const int i = base + g;
-        double s = 0.0;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         if (i < nown) {
             const int kb = (LDG ? __ldg(rp + i) : rp[i]) - rp_base;
             const int ke = (LDG ? __ldg(rp + i + 1) : rp[i + 1]) - rp_base;
-            for (int k = kb + lane; k < ke; k += tpr) {
+            int k = kb + lane;
+            for (; k + 3 * tpr < ke; k += 4 * tpr) {
+                int c[4];
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    c[u] = LDG ? (int)__ldg(col + k + u * tpr) : (int)col[k + u * tpr];
+                    v[u] = LDG ? __ldg(val + k + u * tpr) : val[k + u * tpr];
+                }
+                s0 = fma(v[0], pin[c[0]], s0);
+                s1 = fma(v[1], pin[c[1]], s1);
+                s2 = fma(v[2], pin[c[2]], s2);
+                s3 = fma(v[3], pin[c[3]], s3);
+            }
+            for (; k < ke; k += tpr) {
                 const int c = LDG ? (int)__ldg(col + k) : (int)col[k];
                 const double v = LDG ? __ldg(val + k) : val[k];
-                s = fma(v, pin[c], s);
+                s0 = fma(v, pin[c], s0);
             }
         }
+        double s = (s0 + s1) + (s2 + s3);
         for (int o = tpr >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (i < nown && lane == 0) {
             qout[i] = s;
@@ -179,7 +207,8 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) batch_pcg_kernel(BatchArgs 
     __shared__ int s_job;
     const Team t;
     const BatchSmem L(a.n_max, a.rows_max, a.mat_bytes);
-    double* pfull = reinterpret_cast<double*>(smraw + L.pfull);
+    double* pfull = reinterpret_cast<double*>(smraw + L.pfull);  // p, full length, updated locally
+    double* zfull = reinterpret_cast<double*>(smraw + L.zfull);  // z = D^-1 r, full length, gathered
     double* xo = reinterpret_cast<double*>(smraw + L.x);
     double* ro = reinterpret_cast<double*>(smraw + L.r);
     double* qo = reinterpret_cast<double*>(smraw + L.q);
@@ -197,6 +226,7 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) batch_pcg_kernel(BatchArgs 
         if (j >= a.n_prob) break;
         const int pid = a.order[j];
         const BatchProblem P = a.prob[pid];
+        const unsigned long long t_begin = global_ns();
         const int n = P.n;
         const int r0 = (int)(((long long)n * t.rank) / t.C);
         const int r1 = (int)(((long long)n * (t.rank + 1)) / t.C);
@@ -243,6 +273,10 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) batch_pcg_kernel(BatchArgs 
                 R.iterations = 0;
                 R.rel = -1.0;
                 R.true_rel = -1.0;
+                R.t0 = t_begin;
+                R.t1 = global_ns();
+                R.team = blockIdx.x / t.C;
+                R.pad = 0;
                 a.res[pid] = R;
             }
             t.sync();
@@ -252,7 +286,7 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) batch_pcg_kernel(BatchArgs 
         const int* rp = staged ? srp : gptr + r0;
         const int rp_base = staged ? 0 : kb0;
 
-        // ---- x = 0, r = b, p = z = D^-1 r -----------------------------------
+        // ---- x = 0, r = b, z = D^-1 r (published to every CTA), p = z -------
         double init[2] = {0.0, 0.0};
         for (int i = threadIdx.x; i < nown; i += blockDim.x) {
             const int row = r0 + i;
@@ -268,11 +302,13 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) batch_pcg_kernel(BatchArgs 
             xo[i] = 0.0;
             ro[i] = bi;
             const double zi = di * bi;
-            for (unsigned c = 0; c < t.C; ++c) t.at(pfull, c)[row] = zi;
+            for (unsigned c = 0; c < t.C; ++c) t.at(zfull, c)[row] = zi;
             init[0] += bi * zi;
             init[1] += bi * bi;
         }
-        team_sum<2>(init, sh, slots, SLOT_INIT, t);  // also publishes p
+        team_sum<2>(init, sh, slots, SLOT_INIT, t);  // its barrier also publishes z
+        for (int i = threadIdx.x; i < n; i += blockDim.x) pfull[i] = zfull[i];
+        __syncthreads();
         double rz = init[0];
         double bnorm = sqrt(init[1]);
         if (bnorm == 0.0) bnorm = 1.0;
@@ -298,10 +334,12 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) batch_pcg_kernel(BatchArgs 
                 xo[i] += alpha * pfull[r0 + i];
                 const double ri = ro[i] - alpha * qo[i];
                 ro[i] = ri;
+                const double zi = dio[i] * ri;
+                for (unsigned c = 0; c < t.C; ++c) t.at(zfull, c)[r0 + i] = zi;
                 v2[0] += ri * ri;
-                v2[1] += ri * (dio[i] * ri);
+                v2[1] += ri * zi;
             }
-            team_sum<2>(v2, sh, slots, SLOT_RR, t);
+            team_sum<2>(v2, sh, slots, SLOT_RR, t);  // its barrier also publishes z
             rel = sqrt(v2[0]) / bnorm;
             if (!isfinite(rel)) {
                 status = CUTCELL_E_NAN;
@@ -313,23 +351,22 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) batch_pcg_kernel(BatchArgs 
             }
             const double beta = v2[1] / rz;
             rz = v2[1];
-            for (int i = threadIdx.x; i < nown; i += blockDim.x) {
-                const double pn = dio[i] * ro[i] + beta * pfull[r0 + i];
-                for (unsigned c = 0; c < t.C; ++c) t.at(pfull, c)[r0 + i] = pn;
-            }
-            t.sync();
+            // every CTA forms the whole new p from the gathered z: identical bits
+            // in all copies, and no third barrier for publishing p
+            for (int i = threadIdx.x; i < n; i += blockDim.x) pfull[i] = zfull[i] + beta * pfull[i];
+            __syncthreads();
         }
         const int iters = (k > a.maxiter) ? a.maxiter : k;
 
         // ---- true residual ||b - A x|| / ||b|| in FP64 ------------------------
-        // every CTA has finished its last product with p (a barrier followed it)
+        t.sync();  // every CTA is done reading z before x overwrites it
         for (int i = threadIdx.x; i < nown; i += blockDim.x)
-            for (unsigned c = 0; c < t.C; ++c) t.at(pfull, c)[r0 + i] = xo[i];
+            for (unsigned c = 0; c < t.C; ++c) t.at(zfull, c)[r0 + i] = xo[i];
         t.sync();
         if (staged)
-            spmv_rows<uint16_t, false>(nown, P.tpr_log2, rp, 0, scol, sval, pfull, qo, nullptr);
+            spmv_rows<uint16_t, false>(nown, P.tpr_log2, rp, 0, scol, sval, zfull, qo, nullptr);
         else
-            spmv_rows<int, true>(nown, P.tpr_log2, rp, rp_base, lcol_g, lval_g, pfull, qo, nullptr);
+            spmv_rows<int, true>(nown, P.tpr_log2, rp, rp_base, lcol_g, lval_g, zfull, qo, nullptr);
         __syncthreads();
         double v3[1] = {0.0};
         double* x = a.x + P.vec_off;
@@ -345,6 +382,10 @@ __global__ void __launch_bounds__(BATCH_MAX_THREADS) batch_pcg_kernel(BatchArgs 
             R.iterations = iters;
             R.rel = rel;
             R.true_rel = sqrt(v3[0]) / bnorm;
+            R.t0 = t_begin;
+            R.t1 = global_ns();
+            R.team = blockIdx.x / t.C;
+            R.pad = 0;
             a.res[pid] = R;
         }
         t.sync();  // shared vectors, slots and s_job are reused by the next problem
@@ -664,6 +705,19 @@ int cutcell_batch_solve(cutcell_batch* B, const double* rhs, double* x, double t
         if (R.status == CUTCELL_E_SHAPE) worst = CUTCELL_E_SHAPE;
     }
     return worst;
+}
+
+int cutcell_batch_timeline(const cutcell_batch* B, double* start_us, double* end_us, int32_t* team) {
+    if (!B || !B->exec) return arg_error("batch: no solve has run");
+    unsigned long long t_min = ~0ULL;
+    for (int i = 0; i < B->n_prob; ++i) t_min = std::min(t_min, B->h_res[i].t0);
+    for (int i = 0; i < B->n_prob; ++i) {
+        const BatchResult& R = B->h_res[i];
+        if (start_us) start_us[i] = 1e-3 * (double)(R.t0 - t_min);
+        if (end_us) end_us[i] = 1e-3 * (double)(R.t1 - t_min);
+        if (team) team[i] = R.team;
+    }
+    return CUTCELL_OK;
 }
 
 int cutcell_batch_destroy(cutcell_batch* B) {

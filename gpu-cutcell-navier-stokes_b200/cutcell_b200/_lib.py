@@ -135,6 +135,7 @@ SIGNATURES = {
     "cutcell_batch_configure": (C.c_int, [_P, C.POINTER(CutcellBatchConfig), _P, _P]),
     "cutcell_batch_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "cutcell_batch_solve": (C.c_int, [_P, _P, _P, C.c_double, C.c_int32, C.c_int32, _P, _P]),
+    "cutcell_batch_timeline": (C.c_int, [_P, _P, _P, _P]),
     "cutcell_batch_destroy": (C.c_int, [_P]),
     "cutcell_pcg_solve_csr_noalloc": (
         C.c_int,

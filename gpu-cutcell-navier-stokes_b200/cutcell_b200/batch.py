@@ -50,10 +50,10 @@ def _vec_bytes(n: int) -> int:
 
 
 def fixed_smem(n_max: int, cluster: int) -> int:
-    """Shared-memory bytes per CTA besides the staged matrix: full p, four
+    """Shared-memory bytes per CTA besides the staged matrix: full p and z, four
     row-slice vectors and the reduction slots (the kernel's BatchSmem)."""
     rows = -(-n_max // cluster)
-    return _vec_bytes(n_max) + 4 * _vec_bytes(rows) + _SLOTS
+    return 2 * _vec_bytes(n_max) + 4 * _vec_bytes(rows) + _SLOTS
 
 
 def staging_bytes(cfg: BatchConfig, n_max: int, optin: int = SMEM_OPTIN, per_sm: int = SMEM_PER_SM) -> int:
@@ -221,6 +221,18 @@ class BatchSolver:
         if st not in (_lib.OK, _lib.E_SHAPE):
             _lib.check(st, "cutcell_batch_solve")
         return reps
+
+    def timeline(self) -> dict:
+        """Per-system start / end (microseconds from the first start) and team
+        of the last solve, from the device global timer."""
+        m = self.count
+        t0, t1 = np.zeros(m), np.zeros(m)
+        team = np.zeros(m, dtype=np.int32)
+        _lib.check(
+            self._lib.cutcell_batch_timeline(self._ctx, t0.ctypes.data, t1.ctypes.data, team.ctypes.data),
+            "cutcell_batch_timeline",
+        )
+        return {"start_us": t0, "end_us": t1, "team": team}
 
     def learn_costs(self, reports) -> None:
         """Claim order from the measured work of a solve: nonzeros x iterations."""

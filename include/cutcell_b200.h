@@ -223,6 +223,10 @@ int cutcell_batch_configure(cutcell_batch* batch, const CutcellBatchConfig* cfg,
 int cutcell_batch_info(const cutcell_batch* batch, int32_t* teams, int32_t* smem_bytes);
 int cutcell_batch_solve(cutcell_batch* batch, const double* rhs, double* x, double tol, int32_t maxiter,
                         int32_t precond, CutcellReport* reports, void* stream);
+/* Per-system timeline of the last solve (HOST arrays of n_problems, any may be
+ * NULL): start / end in microseconds from the first system's start (device
+ * global timer) and the team that solved it. */
+int cutcell_batch_timeline(const cutcell_batch* batch, double* start_us, double* end_us, int32_t* team);
 int cutcell_batch_destroy(cutcell_batch* batch);
 
 /* Allocation-free Jacobi-PCG on a device CSR matrix.  No counterpart in the
