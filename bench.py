@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--variants", default="fp64,fp32-ir,bf16-ir,learned")
     ap.add_argument("--train-geometries", type=int, default=3)
     ap.add_argument("--train-pairs", type=int, default=20000)
-    ap.add_argument("--workload", default="sphere", choices=["sphere", "hill"])
+    ap.add_argument("--workload", default="sphere", choices=["sphere", "hill", "hill-step", "batch"])
+    ap.add_argument("--batch-count", type=int, default=72)
     ap.add_argument("--hill-nr", type=int, default=2345)
     ap.add_argument("--hill-nz", type=int, default=32)
     return ap.parse_args()
@@ -147,7 +148,195 @@ def cpu_baseline(prob, ext, b, sample_solves=1):
     return A, float(np.mean(times)), int(its[0]), x
 
 
+BATCH_METRIC = "solves/s: uneven oblique-cut Jacobi-PCG systems solved to rel. residual 1e-9 in one persistent launch"
+
+
+def batch_systems(count: int):
+    """The batched workload: ``count`` 2D oblique cuts (angle U[0,45] deg,
+    offset U(0,h), p in {3,4,5}, n in {6,8,12,16,24}, mass or stiffness),
+    N(0,1) right-hand sides; seeded."""
+    from cutcell_b200 import oblique2d as ob
+
+    cases = ob.sample_cases(count, seed=20260629)
+    systems = [ob.build_oblique(*c).A for c in cases]
+    rng = np.random.default_rng(12345)
+    rhs = [rng.standard_normal(A.shape[0]) for A in systems]
+    return cases, systems, rhs
+
+
+def run_batch_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle.pcg import solve_cpu_cg
+
+    _, systems, rhs = batch_systems(args.batch_count)
+    for _ in range(min(args.warmup, 1)):
+        for A, b in zip(systems, rhs):
+            solve_cpu_cg(A, b, tol=TOL, maxiter=20000)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for A, b in zip(systems, rhs):
+            solve_cpu_cg(A, b, tol=TOL, maxiter=20000)
+        ts.append(time.perf_counter() - t0)
+    v = len(systems) / float(np.mean(ts))
+    line = {
+        "impl": "reference", "metric": BATCH_METRIC, "value": v, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(ts)) * 1e3, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cuts and right-hand sides)",
+        "config": {"workload": f"{len(systems)} oblique 2D cut systems, one solve_cpu_cg each"},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
+                         "sample": f"all {len(systems)} systems per step, sequential SciPy CG"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(args, rank, world, local):
+    """72 uneven systems in one persistent, graph-captured launch (per rank:
+    its longest-processing-time share when several GPUs are used)."""
+    import torch
+
+    from cutcell_b200.batch import BatchSolver, partition_lpt
+    from cutcell_b200.fast_solver_backends import CsrDeviceMatrix
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    t_setup = time.perf_counter()
+    cases, systems, rhs = batch_systems(args.batch_count)
+    t_setup = time.perf_counter() - t_setup
+    costs = [A.nnz * np.sqrt(A.shape[0]) for A in systems]
+    mine = partition_lpt(costs, world)[rank]
+    sys_m = [systems[i] for i in mine]
+    rhs_m = [rhs[i] for i in mine]
+    bs = BatchSolver(sys_m, device=dev)
+    bs.rhs.copy_(torch.from_numpy(bs.packed.pack(rhs_m)))
+    t0 = time.perf_counter()
+    best = bs.autotune(tol=TOL, maxiter=20000)
+    tune_s = time.perf_counter() - t0
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        reps = bs.solve_device(tol=TOL, maxiter=20000)
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        barrier()
+        reps = bs.solve_device(tol=TOL, maxiter=20000)  # device time of the captured graph (CUDA events)
+        ms.append(float(reps[0].elapsed_ms))
+    barrier()
+    clocks = sampler.stop()
+    tot = float(np.sum(ms))
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([tot], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot = float(t.item())
+    ms_step = tot / args.steps
+    value = len(systems) / (ms_step / 1e3)
+    its = np.array([r.iterations for r in reps])
+    ok = all(r.status == 0 and r.true_relative_residual <= 10 * TOL for r in reps)
+    tl = bs.timeline()
+    dur = tl["end_us"] - tl["start_us"]
+    pk = bs.packed
+    bytes_alg = float(np.sum(its * (12.0 * pk.nnz + 13.0 * 8.0 * pk.n)))
+    hbm, hbm_kind = peaks()
+    achieved = bytes_alg / (ms_step / 1e3) / 1e9
+
+    # 72 sequential plain solves through the single-system device path
+    seq_ms, seq_its = 0.0, 0
+    for A, b in zip(sys_m, rhs_m):
+        M = CsrDeviceMatrix(A, device=dev)
+        bd = torch.as_tensor(b).to(dev)
+        M.solve_device(bd, tol=TOL, maxiter=20000)
+        _, r = M.solve_device(bd, tol=TOL, maxiter=20000)
+        seq_ms += float(r.elapsed_ms)
+        seq_its += int(r.iterations)
+        M.close()
+
+    # end to end through the public API: host vectors in (pinned staging, H2D),
+    # host solutions out (D2H), per step
+    for _ in range(2):
+        bs.solve(rhs_m, tol=TOL, maxiter=20000)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out = bs.solve(rhs_m, tol=TOL, maxiter=20000)
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    nvec = int(pk.vec_off[-1])
+    line = {
+        "metric": BATCH_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded cuts and N(0,1) right-hand sides)",
+        "config": {
+            "workload": f"{len(systems)} oblique 2D cut systems (p 3-5, n 6-24, mass/stiffness), Jacobi-PCG to {TOL}",
+            "n_total": int(sum(A.shape[0] for A in systems)), "nnz_total": int(sum(A.nnz for A in systems)),
+            "systems_this_rank": len(sys_m), "autotuned": str(best), "teams": bs.info()["teams"], "tune_s": tune_s,
+            "iterations_total": int(its.sum()), "iterations_max": int(its.max()),
+            "critical_system_us": float(dur.max()), "all_converged": bool(ok), "setup_s": t_setup,
+            "l2": "flushed between timed launches (256 MB write)", "parallelism": f"LPT partition x{world}",
+        },
+        "sequential": {"ms": seq_ms, "solves_per_s": len(sys_m) / (seq_ms / 1e3), "iterations": seq_its,
+                       "path": "one cutcell_pcg_solve (CSR, persistent cooperative launch) per system"},
+        "clocks": clocks,
+        "e2e": {"value": len(systems) / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": 8 * nvec,
+                "d2h_bytes_per_step": 8 * nvec},
+        "gpu_launches": int(args.steps),
+        "roofline": {"bound": "hbm", "kernel": "batch_pcg_kernel (whole batch, one launch)", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": None,
+                     "algorithmic_bytes": bytes_alg,
+                     "note": "algorithmic bytes per iteration 12 nnz + 13*8 n; the CSR slices and vectors are held in shared memory"},
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        from oracle.pcg import solve_cpu_cg
+
+        t0 = time.perf_counter()
+        k = 0
+        while k < len(systems) and time.perf_counter() - t0 < 20.0:
+            solve_cpu_cg(systems[k], rhs[k], tol=TOL, maxiter=20000)
+            k += 1
+        cs = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": k / cs, "unit": "solves/s", "cores": 1, "kind": "port",
+                                "sample": f"first {k} of the {len(systems)} systems, sequential SciPy CG"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    bs.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def run_reference(args, rank, world):
+    if args.workload == "batch":
+        return run_batch_reference(args, rank, world)
     if rank != 0:
         return 0
     nth = os.cpu_count() or 1
@@ -254,6 +443,87 @@ def run_hill(args, rank, world, local):
     return 0
 
 
+def run_hill_step(args, rank, world, local):
+    """One hill_fastdiag_step (SSP-RK3 skew advection + fast-diagonalisation
+    solve) at the channel configuration's sizes: nr = 2345 reduced 2D modes
+    (64 x 32 elements, p = 3), nz = 32, 64 x 32 cells of 14 x 14 Gauss points
+    (n2q = 401,408) with 16 modes per sample row, 9 z points per element.
+    Sample machinery and operators are seeded synthetic stand-ins of those
+    shapes (the reference builds them in hours on the CPU)."""
+    import torch
+
+    from cutcell_b200.hill import FastDiagHill, HillAdvection, synthetic_machinery
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    nr, nz = args.hill_nr, args.hill_nz
+    t0 = time.perf_counter()
+    m = synthetic_machinery(nr=nr, nz=nz, cells=(64, 32), pts_per_cell=196, modes_per_row=16)
+    adv = HillAdvection(m["phi"], m["dpx"], m["dpy"], m["w2"], m["Vz"], m["dVz"], m["wz"], m["M2inv"], m["Mzinv"],
+                        device=dev)
+    g = torch.Generator(device=dev).manual_seed(20260629)
+    rnd = lambda *shape: torch.randn(*shape, generator=g, device=dev, dtype=torch.float64) / np.sqrt(shape[-1])
+    M2, Qx2, Qy2 = rnd(nr, nr), rnd(nr, nr), rnd(nr, nr)
+    Mz_row = np.zeros(nz); Mz_row[0], Mz_row[1], Mz_row[-1] = 0.6, 0.2, 0.2
+    Sz_row = np.zeros(nz); Sz_row[0], Sz_row[1], Sz_row[-1] = 2.0, -1.0, -1.0
+    Kz_row = np.zeros(nz); Kz_row[1], Kz_row[-1] = 0.5, -0.5
+    Ainv, Sinv = rnd(nz, nr, nr), rnd(nz, nr, nr)
+    fd = FastDiagHill(device=dev).build(M2, Qx2, Qy2, None, Mz_row, Sz_row, Kz_row, 0.01, inverses=(Ainv, Sinv))
+    setup_s = time.perf_counter() - t0
+    u0 = [0.1 * rnd(nr, nz) for _ in range(3)]
+    u = [t.clone() for t in u0]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        for a, b in zip(u, u0):
+            a.copy_(b)
+        adv.step(fd, u, 0.02, 0.7)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms, ms_adv = [], []
+    for _ in range(args.steps):
+        for a, b in zip(u, u0):
+            a.copy_(b)
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        adv.step(fd, u, 0.02, 0.7)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0.record()
+        adv.skew_conv(*u0)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_adv.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    t = float(np.mean(ms))
+    ta = float(np.mean(ms_adv))
+    n2q, nzq = m["phi"].shape[0], m["Vz"].shape[0]
+    L = m["phi"].nnz // n2q
+    # FP64 flops of one skew_conv of three components (fused kernel), per 2D point:
+    # 2D sample 9 L nz FMA, z band 3 x (qpe x nz) x (48 + 12 FMA + ~10), 2D load 9 L nz FMA
+    flop_adv = 2.0 * n2q * (18 * L * nz + 3 * nzq * 70) + 2.0 * nr * nr * 3 * nz
+    line = {
+        "metric": "ms per hill fast step (SSP-RK3 skew advection + fast-diagonalisation solve)",
+        "value": t, "unit": "ms/step", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic sample machinery and operators of the configuration's sizes (seeded)",
+        "config": {"workload": f"hill fast step nr={nr} nz={nz} n2q={n2q} nzq={nzq} row_nnz={L}",
+                   "l2": "flushed between timed steps", "setup_s": setup_s, "advect_ms": ta,
+                   "advect_gflops": flop_adv / (ta * 1e-3) / 1e9},
+        "clocks": clocks, "gpu_launches": (3 * 4 + 3 + 15) * args.steps,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    adv.close()
+    fd.close()
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -261,6 +531,10 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "hill":
         return run_hill(args, rank, world, local)
+    if args.workload == "batch":
+        return run_batch(args, rank, world, local)
+    if args.workload == "hill-step":
+        return run_hill_step(args, rank, world, local)
     import torch
 
     torch.cuda.set_device(local)

@@ -97,6 +97,16 @@ class CutcellTileDesc(C.Structure):
     ]
 
 
+class CutcellHillDesc(C.Structure):
+    _fields_ = [(f, C.c_int32) for f in ("nr", "nz", "qpe", "nzb", "n_seg", "lmax", "n_part", "n2q")] + [
+        (f, _P)
+        for f in (
+            "seg_q0", "seg_q1", "seg_pat", "seg_len", "pat_idx", "sp_ptr", "phi", "dpx", "dpy", "w2", "zb", "Vl",
+            "dVl", "wzl", "g_ptr", "g_ent", "Mzinv", "M2inv",
+        )
+    ]
+
+
 class CutcellBatchConfig(C.Structure):
     _fields_ = [
         ("cluster", C.c_int32),
@@ -131,6 +141,10 @@ SIGNATURES = {
     "cutcell_fastdiag_create": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "cutcell_fastdiag_solve": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
     "cutcell_fastdiag_destroy": (C.c_int, [_P]),
+    "cutcell_hill_create": (C.c_int, [C.POINTER(CutcellHillDesc), C.POINTER(_P)]),
+    "cutcell_hill_skew_conv": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
+    "cutcell_hill_step": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, C.c_double, _P]),
+    "cutcell_hill_destroy": (C.c_int, [_P]),
     "cutcell_batch_create": (C.c_int, [C.c_int32, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "cutcell_batch_configure": (C.c_int, [_P, C.POINTER(CutcellBatchConfig), _P, _P]),
     "cutcell_batch_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),

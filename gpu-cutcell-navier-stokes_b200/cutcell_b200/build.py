@@ -17,7 +17,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = ROOT / "csrc"
-SOURCES = ["cutcell.cu", "noalloc.cu", "batch.cu"]
+SOURCES = ["cutcell.cu", "noalloc.cu", "batch.cu", "hilladv.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -110,3 +110,201 @@ class FastDiagHill:
             self.close()
         except Exception:
             pass
+
+
+# ---- advection (hill_skew_conv) and the fast step (hill_fastdiag_step) ----
+
+
+def z_element_tables(Vz, dVz, wz, nz):
+    """Per z element: its (p+1) basis functions in periodic order and their
+    values / derivatives at the element's quadrature points.
+
+    The z quadrature nodes are grouped by element (cpp/include/cut/hill3d.h:
+    153-160: element e owns nodes e*qpe .. e*qpe+qpe-1).  The band of element e
+    must be the periodic run (e - s + j) mod nz, j = 0..nzb-1, with the same
+    shift s for every element (uniform periodic B-splines), so that element e
+    writes mode (e - s + j) mod nz in scatter round j without conflicts."""
+    Vz, dVz, wz = np.asarray(Vz), np.asarray(dVz), np.asarray(wz)
+    nzq = Vz.shape[0]
+    qpe = nzq // nz
+    if qpe * nz != nzq:
+        raise ValueError("z quadrature is not a whole number of points per element")
+    bands = []
+    for e in range(nz):
+        rows = slice(e * qpe, (e + 1) * qpe)
+        cols = np.nonzero((np.abs(Vz[rows]) + np.abs(dVz[rows])).sum(0))[0]
+        k = cols.size
+        start = None
+        for c0 in cols:
+            if {int((c0 + j) % nz) for j in range(k)} == set(int(c) for c in cols):
+                start = int(c0)
+                break
+        if start is None:
+            raise ValueError(f"z element {e}: basis functions are not a periodic run")
+        bands.append([(start + j) % nz for j in range(k)])
+    nzb = len(bands[0])
+    shifts = {(e - b[0]) % nz for e, b in enumerate(bands)}
+    if any(len(b) != nzb for b in bands) or len(shifts) != 1:
+        raise ValueError("z bands are not a uniform periodic shift")
+    zb = np.array(bands, dtype=np.int32)
+    Vl = np.stack([Vz[e * qpe : (e + 1) * qpe][:, zb[e]] for e in range(nz)])
+    dVl = np.stack([dVz[e * qpe : (e + 1) * qpe][:, zb[e]] for e in range(nz)])
+    wzl = wz.reshape(nz, qpe)
+    return zb, Vl, dVl, wzl, qpe
+
+
+def segment_tables(ptr, idx, seg_max=128):
+    """Segments of consecutive 2D points whose sample rows have the same mode
+    pattern (at most seg_max points each), their patterns, and for every
+    reduced mode the partial rows (segment pattern slots) that feed it, in
+    segment order."""
+    ptr = np.asarray(ptr, dtype=np.int64)
+    idx = np.asarray(idx, dtype=np.int64)
+    n2q = ptr.size - 1
+    q0s, q1s, pats = [], [], []
+    q = 0
+    while q < n2q:
+        pat = idx[ptr[q] : ptr[q + 1]]
+        r = q + 1
+        while r < n2q and r - q < seg_max and ptr[r + 1] - ptr[r] == pat.size and np.array_equal(idx[ptr[r] : ptr[r + 1]], pat):
+            r += 1
+        q0s.append(q)
+        q1s.append(r)
+        pats.append(pat)
+        q = r
+    seg_len = np.array([p.size for p in pats], dtype=np.int32)
+    seg_pat = np.concatenate([[0], np.cumsum(seg_len)[:-1]]).astype(np.int32)
+    pat_idx = np.concatenate(pats).astype(np.int32)
+    order = np.argsort(pat_idx, kind="stable")  # by mode, then by partial row (segment order)
+    nr = int(pat_idx.max()) + 1 if pat_idx.size else 0
+    g_ptr = np.zeros(nr + 1, dtype=np.int32)
+    np.add.at(g_ptr, pat_idx + 1, 1)
+    g_ptr = np.cumsum(g_ptr).astype(np.int32)
+    return {
+        "seg_q0": np.array(q0s, np.int32), "seg_q1": np.array(q1s, np.int32), "seg_pat": seg_pat,
+        "seg_len": seg_len, "pat_idx": pat_idx, "g_ptr": g_ptr, "g_ent": order.astype(np.int32),
+    }
+
+
+class HillAdvection:
+    """Device advection of the periodic hill (hill_skew_conv of all three
+    components) and the fast step, from Hill3D's sample machinery.
+
+    ``phi, dpx, dpy``: scipy CSR (n2q x nr) sample rows on one pattern
+    (sp_idx / sp_phi / sp_dpx / sp_dpy); ``w2`` (n2q); ``Vz, dVz`` (nzq x nz);
+    ``wz`` (nzq); ``M2inv`` (nr x nr), ``Mzinv`` (nz x nz)."""
+
+    def __init__(self, phi, dpx, dpy, w2, Vz, dVz, wz, M2inv, Mzinv, device="cuda", seg_max=128):
+        import torch
+
+        self._lib = _lib.load()
+        self.device = torch.device(device)
+        phi, dpx, dpy = phi.tocsr(), dpx.tocsr(), dpy.tocsr()
+        for other in (dpx, dpy):
+            if not (np.array_equal(other.indptr, phi.indptr) and np.array_equal(other.indices, phi.indices)):
+                raise ValueError("phi, dpx and dpy must share one sparsity pattern")
+        self.n2q, self.nr = phi.shape
+        self.nz = int(np.asarray(Vz).shape[1])
+        zb, Vl, dVl, wzl, qpe = z_element_tables(Vz, dVz, wz, self.nz)
+        seg = segment_tables(phi.indptr, phi.indices, seg_max)
+        if seg["g_ptr"].size - 1 < self.nr:
+            seg["g_ptr"] = np.concatenate([seg["g_ptr"], np.full(self.nr + 1 - seg["g_ptr"].size, seg["g_ptr"][-1], np.int32)])
+        self.tables = seg
+        dv = self.device
+        ti = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32)).to(dv)
+        tf = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(dv)
+        self._t = {
+            **{k: ti(v) for k, v in seg.items()},
+            "sp_ptr": ti(phi.indptr), "phi": tf(phi.data), "dpx": tf(dpx.data), "dpy": tf(dpy.data), "w2": tf(w2),
+            "zb": ti(zb), "Vl": tf(Vl), "dVl": tf(dVl), "wzl": tf(wzl), "Mzinv": tf(Mzinv), "M2inv": tf(M2inv),
+        }
+        T = self._t
+        desc = _lib.CutcellHillDesc(
+            self.nr, self.nz, int(qpe), int(zb.shape[1]), int(seg["seg_len"].size), int(seg["seg_len"].max()),
+            int(seg["pat_idx"].size), int(self.n2q),
+            *(T[k].data_ptr() for k in ("seg_q0", "seg_q1", "seg_pat", "seg_len", "pat_idx", "sp_ptr", "phi", "dpx",
+                                        "dpy", "w2", "zb", "Vl", "dVl", "wzl", "g_ptr", "g_ent", "Mzinv", "M2inv")),
+        )
+        ctx = C.c_void_p()
+        _lib.check(self._lib.cutcell_hill_create(C.byref(desc), C.byref(ctx)), "cutcell_hill_create")
+        self._ctx = ctx
+
+    def _fields(self, u):
+        import torch
+
+        return [torch.as_tensor(c, dtype=torch.float64, device=self.device).contiguous() for c in u]
+
+    def skew_conv(self, ux, uy, uz):
+        """hill_skew_conv(w = u, u_c) for the three components (device tensors)."""
+        import torch
+
+        ins = self._fields((ux, uy, uz))
+        outs = [torch.empty_like(ins[0]) for _ in range(3)]
+        _lib.check(
+            self._lib.cutcell_hill_skew_conv(self._ctx, *(t.data_ptr() for t in ins), *(o.data_ptr() for o in outs),
+                                             _lib.current_stream_ptr()),
+            "cutcell_hill_skew_conv",
+        )
+        return outs
+
+    def step(self, fd: "FastDiagHill", u, dt: float, fx: float = 0.0):
+        """hill_fastdiag_step in place on the three device fields ``u``."""
+        _lib.check(
+            self._lib.cutcell_hill_step(self._ctx, fd._ctx, *(t.data_ptr() for t in u), float(dt), float(fx),
+                                        _lib.current_stream_ptr()),
+            "cutcell_hill_step",
+        )
+        return u
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.cutcell_hill_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cubic_bspline(t):
+    """Centred cardinal cubic B-spline and its derivative (support |t| < 2)."""
+    a = np.abs(t)
+    v = np.where(a < 1, 2.0 / 3.0 - a**2 + 0.5 * a**3, np.where(a < 2, (2.0 - a) ** 3 / 6.0, 0.0))
+    dv = np.where(a < 1, -2.0 * a + 1.5 * a**2, np.where(a < 2, -0.5 * (2.0 - a) ** 2, 0.0)) * np.sign(t)
+    return v, dv
+
+
+def synthetic_machinery(nr=2345, nz=32, cells=(64, 32), pts_per_cell=196, modes_per_row=16, Lz=4.5, seed=20260629):
+    """Seeded stand-in for Hill3D's sample machinery at a given size: each 2D
+    cell's points share one pattern of ``modes_per_row`` reduced modes (a
+    window of the mode range moving with the cell), values and weights are
+    random; the z basis is the periodic cubic B-spline on nz elements with
+    9 Gauss points each.  Used for timing and for device-vs-oracle checks
+    where the reference machinery is not available."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    ncell = cells[0] * cells[1]
+    n2q = ncell * pts_per_cell
+    starts = (np.arange(ncell) * (nr - modes_per_row)) // max(ncell - 1, 1)
+    cols = (starts[:, None] + np.arange(modes_per_row)[None, :])
+    idx = np.repeat(cols, pts_per_cell, axis=0).ravel()
+    ptr = np.arange(n2q + 1) * modes_per_row
+    mk = lambda scale: sp.csr_matrix((rng.standard_normal(idx.size) * scale, idx, ptr), shape=(n2q, nr))
+    phi, dpx, dpy = mk(0.3), mk(2.0), mk(2.0)
+    w2 = rng.uniform(0.5, 1.5, n2q) / n2q
+    hz = Lz / nz
+    g, gw = np.polynomial.legendre.leggauss(9)
+    zq = ((np.arange(nz)[:, None] + 0.5 * (g[None, :] + 1.0)) * hz).ravel()
+    wz = np.tile(0.5 * gw * hz, nz)
+    d = zq[:, None] - hz * np.arange(nz)[None, :]
+    d -= Lz * np.floor(d / Lz + 0.5)
+    Vz, dVz = cubic_bspline(d / hz)
+    dVz = dVz / hz
+    A = rng.standard_normal((nr, nr)) / np.sqrt(nr)
+    M2inv = np.eye(nr) + 0.1 * (A + A.T)
+    Mzinv = np.eye(nz) + 0.05 * np.roll(np.eye(nz), 1, 1) + 0.05 * np.roll(np.eye(nz), -1, 1)
+    return {"phi": phi, "dpx": dpx, "dpy": dpy, "w2": w2, "Vz": Vz, "dVz": dVz, "wz": wz, "M2inv": M2inv,
+            "Mzinv": Mzinv, "nr": nr, "nz": nz}

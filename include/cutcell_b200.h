@@ -182,6 +182,52 @@ int cutcell_fastdiag_solve(cutcell_fastdiag* fd, const double* ux, const double*
                            double* oy, double* oz, void* stream);
 int cutcell_fastdiag_destroy(cutcell_fastdiag* fd);
 
+/* ---- periodic-hill advection and fast step ----
+ * hill_skew_conv (cpp/include/cut/hill3d.h:519-538) for all three velocity
+ * components, and hill_fastdiag_step (cpp/include/cut/hill_fastdiag.h:83-95).
+ * The descriptor holds device pointers to the Galerkin sample machinery of
+ * Hill3D (hill3d.h:86-93: sparse reduced 2D sample rows sp_idx / sp_phi /
+ * sp_dpx / sp_dpy, weights w2; z basis Vz, dVz, weights wz) in the blocked
+ * form the host prepares (cutcell_b200/hill.py, HillAdvection): segments of
+ * consecutive 2D points sharing one row pattern, per-z-element band tables,
+ * and the per-mode gather of segment partials; plus the mass inverses M2inv
+ * (nr x nr) and Mzinv (nz x nz).  Supported: nz <= 32, z degree 3 (band 4),
+ * <= 16 z points per element, <= 32 modes per 2D row pattern. */
+typedef struct {
+    int32_t nr, nz;        /* reduced 2D modes, z modes */
+    int32_t qpe, nzb;      /* z quadrature points per z element, z band width */
+    int32_t n_seg, lmax;   /* segments, longest row pattern */
+    int32_t n_part, n2q;   /* sum of pattern lengths, 2D quadrature points */
+    const int32_t* seg_q0;   /* [n_seg] */
+    const int32_t* seg_q1;   /* [n_seg] */
+    const int32_t* seg_pat;  /* [n_seg] offset of the pattern in pat_idx */
+    const int32_t* seg_len;  /* [n_seg] */
+    const int32_t* pat_idx;  /* [n_part] reduced modes */
+    const int32_t* sp_ptr;   /* [n2q + 1] */
+    const double* phi;       /* sample row values, aligned with the patterns */
+    const double* dpx;
+    const double* dpy;
+    const double* w2;        /* [n2q] */
+    const int32_t* zb;       /* [nz][nzb] modes of each z element in periodic order */
+    const double* Vl;        /* [nz][qpe][nzb] */
+    const double* dVl;       /* [nz][qpe][nzb] */
+    const double* wzl;       /* [nz][qpe] */
+    const int32_t* g_ptr;    /* [nr + 1] */
+    const int32_t* g_ent;    /* [n_part] partial rows of each mode, segment order */
+    const double* Mzinv;
+    const double* M2inv;
+} CutcellHillDesc;
+typedef struct cutcell_hill cutcell_hill;
+int cutcell_hill_create(const CutcellHillDesc* desc, cutcell_hill** out);
+/* (cx, cy, cz) = hill_skew_conv(w = u, u_c) for c = x, y, z; FieldH arrays. */
+int cutcell_hill_skew_conv(cutcell_hill* hill, const double* ux, const double* uy, const double* uz, double* cx,
+                           double* cy, double* cz, void* stream);
+/* One hill_fastdiag_step in place on (ux, uy, uz): SSP-RK3 of -skew_conv,
+ * + dt fx on ux, then cutcell_fastdiag_solve. */
+int cutcell_hill_step(cutcell_hill* hill, cutcell_fastdiag* fd, double* ux, double* uy, double* uz, double dt,
+                      double fx, void* stream);
+int cutcell_hill_destroy(cutcell_hill* hill);
+
 /* ---- batched persistent Jacobi-PCG over many uneven systems ----
  * Replaces the one-system-at-a-time loop of the reference's solver sweeps
  * (code/fast_solver_workbench.py:169-176 calling solve_cpu_cg / solve_gpu_cg,

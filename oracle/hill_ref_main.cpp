@@ -60,6 +60,39 @@ int main(int argc, char** argv) {
     put(f, out[0].v);
     put(f, out[1].v);
     put(f, out[2].v);
+    // the Galerkin sample / load machinery (hill3d.h:86-93) and the mass inverses
+    {
+        double dims[2] = {(double)H.n2q, (double)H.nzq};
+        fwrite(dims, sizeof(double), 2, f);
+        std::vector<double> ptr(H.n2q + 1, 0.0), idx, phi, dpx, dpy;
+        for (int q = 0; q < H.n2q; ++q) {
+            ptr[q + 1] = ptr[q] + (double)H.sp_idx[q].size();
+            for (size_t a = 0; a < H.sp_idx[q].size(); ++a) {
+                idx.push_back((double)H.sp_idx[q][a]);
+                phi.push_back(H.sp_phi[q][a]);
+                dpx.push_back(H.sp_dpx[q][a]);
+                dpy.push_back(H.sp_dpy[q][a]);
+            }
+        }
+        double nnz = (double)idx.size();
+        fwrite(&nnz, sizeof(double), 1, f);
+        put(f, ptr);
+        put(f, idx);
+        put(f, phi);
+        put(f, dpx);
+        put(f, dpy);
+        put(f, H.w2);
+        put(f, H.Vz.a);
+        put(f, H.dVz.a);
+        put(f, H.wz);
+        put(f, H.M2inv.a);
+        put(f, H.Mzinv.a);
+        // one skew-symmetric convection of each component by the sampled field
+        QField wx = hill_sample(H, s.ux), wy = hill_sample(H, s.uy), wz = hill_sample(H, s.uz);
+        put(f, hill_skew_conv(H, wx, wy, wz, s.ux).v);
+        put(f, hill_skew_conv(H, wx, wy, wz, s.uy).v);
+        put(f, hill_skew_conv(H, wx, wy, wz, s.uz).v);
+    }
     if (steps > 0) {
         HillNS st = s;
         for (int k = 0; k < steps; ++k) hill_fastdiag_step(H, fd, st, dt, fx);
