@@ -93,6 +93,12 @@ __device__ __forceinline__ double grid_reduce(const double* part, int nblocks, d
     return block_sum(s, sh);
 }
 
+// p_new = D^-1 r + beta p_old with one fixed rounding sequence, so a value
+// formed on the fly is bit-identical to the stored one.
+__device__ __forceinline__ double p_next(double dinv, double r, double beta, double pold) {
+    return __fma_rn(beta, pold, __dmul_rn(dinv, r));
+}
+
 template <typename T> struct Conv;
 template <> struct Conv<double> {
     typedef double acc;

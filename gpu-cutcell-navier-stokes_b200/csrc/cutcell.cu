@@ -143,6 +143,7 @@ struct cutcell_ctx {
     bool use_jacobi = true;
     double* r = nullptr;
     double* p = nullptr;
+    double* p2 = nullptr;
     double* Ap = nullptr;
     double* d = nullptr;
     double* rhat = nullptr;
@@ -169,6 +170,7 @@ static int alloc_scratch(cutcell_ctx* c) {
     fill_kernel<<<ceil_div(c->n, 256), 256>>>(c->n, 1.0, c->ones);
     CK(cudaMalloc(&c->r, nb));
     CK(cudaMalloc(&c->p, nb));
+    CK(cudaMalloc(&c->p2, nb));
     CK(cudaMalloc(&c->Ap, nb));
     CK(cudaMalloc(&c->d, nb));
     CK(cudaMalloc(&c->rhat, nb));
@@ -209,6 +211,7 @@ static PcgBufs make_bufs(cutcell_ctx* c) {
     B.p = c->p;
     B.Ap = c->Ap;
     B.part = c->part;
+    B.p2 = c->p2;
     return B;
 }
 
@@ -371,7 +374,8 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     const int p = t->degree, P1 = p + 1, P = P1 * P1 * P1, D = t->tile + p;
     const int nb = t->n_elements + p;
     if (p < 1 || p > 5 || t->tile != 4 || t->n_tiles_axis * t->tile < t->n_elements ||
-        (long)nb * nb * nb != t->n_full || t->n_red <= 0 || t->cut_chunk < 1)
+        (long)nb * nb * nb != t->n_full || t->n_red <= 0 || t->cut_chunk < 1 || t->n_mixed < 0 ||
+        t->n_mixed > t->n_items)
         return CUTCELL_E_SHAPE;
     cutcell_ctx* c = new cutcell_ctx();
     c->kind = KIND_TILES;
@@ -418,6 +422,15 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     d.nta = t->n_tiles_axis;
     d.nb = nb;
     d.n_items = t->n_items;
+    d.n_mixed = t->n_mixed;
+    {
+        // warp-level full tiles pay off once there are many per SM
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        d.full_warp = (t->n_items - t->n_mixed) >= 8 * (sms > 0 ? sms : 148) ? 1 : 0;
+        // one thread per DOF once there are more than about two per thread of a 2 x 256 x SMs grid
+        d.lane1 = t->n_need > 2 * 512 * (sms > 0 ? sms : 148) ? 1 : 0;
+    }
     d.n_cut = t->n_cut;
     d.cut_chunk = t->cut_chunk;
     d.a_mass = t->a_mass;
@@ -557,7 +570,7 @@ int cutcell_destroy(cutcell_ctx* c) {
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
     void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
-                    c->p,     c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
+                    c->p,     c->p2,    c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (c->ev0) cudaEventDestroy(c->ev0);

@@ -20,6 +20,7 @@
 
 template <typename V>
 struct CsrOp {
+    static constexpr bool kFusedP = false;
     int n;
     int tpr_log2;  // threads per row = 1 << tpr_log2 (1..32)
     const int* __restrict__ ptr;
@@ -88,6 +89,25 @@ struct ExtDev {
         }
     }
 
+    // psmall[s] = E[small s, :] p_new with p_new = D^-1 r + beta p_old formed
+    // on the fly (the stored p_new is being written concurrently)
+    __device__ __forceinline__ void small_rows_next(const double* pold, const double* r, const double* dinv,
+                                                    double beta) const {
+        const int lane = threadIdx.x & 31;
+        const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const int nw = (gridDim.x * blockDim.x) >> 5;
+        for (int s = gw; s < n_small; s += nw) {
+            double acc = 0.0;
+            const int k1 = __ldg(small_ptr + s + 1);
+            for (int k = __ldg(small_ptr + s) + lane; k < k1; k += 32) {
+                const int j = __ldg(small_idx + k);
+                acc += __ldg(small_val + k) * p_next(__ldg(dinv + j), __ldcg(r + j), beta, __ldcg(pold + j));
+            }
+            acc = warp_sum(acc);
+            if (lane == 0) psmall[s] = acc;
+        }
+    }
+
     // (E x)_i once small_rows(x) has completed grid-wide
     __device__ __forceinline__ double gather_fast(const double* x, int i) const {
         const int r = __ldg(red_of_full + i);
@@ -133,7 +153,10 @@ enum { TILE_EMPTY = 0, TILE_FULL = 1, TILE_MIXED = 2 };
 // Non-templated description shared by every precision / degree instance.
 struct TileData {
     int n, p, T, nta, nb;
-    int n_items;      // work items (tiles and cut chunks, heaviest first)
+    int n_items;      // tile work items: mixed tiles (heaviest first), then full tiles
+    int n_mixed;      // leading mixed-tile items; the rest are full tiles
+    int full_warp;    // 1: full tiles are warp-level items (many per SM); 0: block-level
+    int lane1;        // 1: one thread per DOF / row in phase 2 (many per thread); 0: groups of 4 lanes
     int n_cut;
     int cut_chunk;    // cut elements per work item
     double a_mass;
@@ -163,6 +186,7 @@ struct TileData {
 
 template <typename CT, int P1>
 struct TileOp {
+    static constexpr bool kFusedP = true;
     static constexpr int P = P1 * P1 * P1;
     static constexpr int PP = P1 * P1;
     static constexpr int T = 4;
@@ -176,12 +200,15 @@ struct TileOp {
     TileData td;
     const CT* __restrict__ cut_mats;
 
+    // per-warp region of a warp-level item: a full tile's window and three
+    // pass buffers, or a cut element's gathered values
+    static constexpr int WS = (4 * D3a > Pa) ? 4 * D3a : Pa;
     static size_t smem_bytes() {
-        const size_t full = 5 * (size_t)D3a;
         const size_t mixed = (size_t)D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa + 3 * 4 * 2 * PP;
-        const size_t cut = (size_t)NW * Pa;
-        size_t m = full > mixed ? full : mixed;
-        return (CTRL + (m > cut ? m : cut)) * sizeof(double);
+        const size_t full = 5 * (size_t)D3a;
+        const size_t warp = (size_t)NW * WS;
+        size_t m = mixed > warp ? mixed : warp;
+        return (CTRL + (m > full ? m : full)) * sizeof(double);
     }
 
     __device__ __forceinline__ void gather_window(const double* pred, int tx, int ty, int tz, double* xs) const {
@@ -195,6 +222,7 @@ struct TileOp {
         }
     }
 
+    // A full tile by the whole block (few tiles per block: latency matters).
     __device__ void full_tile(int tx, int ty, int tz, double* xs, double* out) const {
         double* u1 = xs + D3a;
         double* u2 = u1 + D3a;
@@ -254,6 +282,119 @@ struct TileOp {
             }
             out[k] = s;
         }
+    }
+
+    // A full tile by one warp: E-gather of the D^3 window, then the x, y, z
+    // banded passes with __syncwarp between them (no block barrier), so a
+    // block has NW tiles in flight.  Every per-lane loop has a compile-time
+    // trip count (KPL entries) and is unrolled, so a lane's loads are all in
+    // flight together instead of one entry's latency after another.
+    // ws: 4 * D3a doubles.
+    static constexpr int KPL = (D3 + 31) / 32;
+    __device__ void full_tile_warp(const double* pred, int tile, double* ws) const {
+        const int lane = threadIdx.x & 31;
+        const int nta = td.nta, nb = td.nb;
+        const int tx = tile % nta, ty = (tile / nta) % nta, tz = tile / (nta * nta);
+        double* xs = ws;
+        double* u1 = ws + D3a;
+        double* u2 = u1 + D3a;
+        double* v2 = u2 + D3a;
+        double* v1 = xs;  // the window is dead after the x pass
+        {
+            int gi[KPL];
+#pragma unroll
+            for (int t = 0; t < KPL; ++t) {
+                const int k = lane + 32 * t;
+                const int dx = k % D, dy = (k / D) % D, dz = k / (D * D);
+                const int gx = tx * T + dx, gy = ty * T + dy, gz = tz * T + dz;
+                gi[t] = (k < D3 && gx < nb && gy < nb && gz < nb) ? (gz * nb + gy) * nb + gx : -1;
+            }
+            int rr[KPL];
+#pragma unroll
+            for (int t = 0; t < KPL; ++t) rr[t] = gi[t] >= 0 ? __ldg(td.ext.red_of_full + gi[t]) : -1;
+            double xv[KPL];
+#pragma unroll
+            for (int t = 0; t < KPL; ++t) {
+                if (rr[t] >= 0)
+                    xv[t] = __ldcg(pred + rr[t]);
+                else if (gi[t] >= 0) {
+                    const int sl = __ldg(td.ext.small_slot + gi[t]);
+                    xv[t] = sl >= 0 ? __ldcg(td.ext.psmall + sl) : 0.0;
+                } else
+                    xv[t] = 0.0;
+            }
+#pragma unroll
+            for (int t = 0; t < KPL; ++t)
+                if (lane + 32 * t < D3) xs[lane + 32 * t] = xv[t];
+        }
+        __syncwarp();
+        const double* Mx = td.TM + (size_t)tx * D * D;
+        const double* Ax = td.TA + (size_t)tx * D * D;
+        const double* My = td.TM + (size_t)ty * D * D;
+        const double* Ky = td.TK + ((size_t)1 * nta + ty) * D * D;
+        const double* Mz = td.TM + (size_t)tz * D * D;
+        const double* Kz = td.TK + ((size_t)2 * nta + tz) * D * D;
+        constexpr int p = P1 - 1;
+#pragma unroll
+        for (int t = 0; t < KPL; ++t) {
+            const int k = lane + 32 * t;
+            if (k < D3) {
+                const int i = k % D, row = k - i;
+                double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int o = -p; o <= p; ++o) {
+                    const int j = i + o;
+                    if (j >= 0 && j < D) {
+                        const double xv = xs[row + j];
+                        s1 += __ldg(Mx + i * D + j) * xv;
+                        s2 += __ldg(Ax + i * D + j) * xv;
+                    }
+                }
+                u1[k] = s1;
+                u2[k] = s2;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < KPL; ++t) {
+            const int k = lane + 32 * t;
+            if (k < D3) {
+                const int x = k % D, i = (k / D) % D, z = k / (D * D);
+                double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                for (int o = -p; o <= p; ++o) {
+                    const int j = i + o;
+                    if (j >= 0 && j < D) {
+                        const int q = (z * D + j) * D + x;
+                        const double m = __ldg(My + i * D + j);
+                        s1 += m * u1[q];
+                        s2 += m * u2[q] + __ldg(Ky + i * D + j) * u1[q];
+                    }
+                }
+                v1[k] = s1;
+                v2[k] = s2;
+            }
+        }
+        __syncwarp();
+        double* out = td.ypart + (size_t)tile * D3;
+#pragma unroll
+        for (int t = 0; t < KPL; ++t) {
+            const int k = lane + 32 * t;
+            if (k < D3) {
+                const int xy = k % (D * D), i = k / (D * D);
+                double s = 0.0;
+#pragma unroll
+                for (int o = -p; o <= p; ++o) {
+                    const int j = i + o;
+                    if (j >= 0 && j < D) {
+                        const int q = j * D * D + xy;
+                        s += __ldg(Mz + i * D + j) * v2[q] + __ldg(Kz + i * D + j) * v1[q];
+                    }
+                }
+                out[k] = s;
+            }
+        }
+        __syncwarp();
     }
 
     __device__ void mixed_tile(int tile, int tx, int ty, int tz, double* xs, double* out) const {
@@ -390,41 +531,81 @@ struct TileOp {
         unsigned* dbgw = nullptr;
 #endif
         (void)dbgw;
+        // block-level items: mixed tiles, and the full tiles unless they are warp-level
+        const int n_block_items = td.full_warp ? td.n_mixed : td.n_items;
         while (true) {
             if (threadIdx.x == 0) s_item = (int)atomicAdd(td.work, 1u);
             __syncthreads();
             const int item = s_item;
             __syncthreads();
-            if (item >= td.n_items) break;
+            if (item >= n_block_items) break;
             if (!CUTCELL_OK_IF(item >= 0, 8, item, (td.work + 64))) break;
-            const int code = __ldg(td.item_list + item);
-            if (code >= 0) {
-                const int tile = code;
-                const int nta = td.nta;
-                if (!CUTCELL_OK_IF(tile < nta * nta * nta, 9, tile, (td.work + 64))) continue;
-                const int tx = tile % nta, ty = (tile / nta) % nta, tz = tile / (nta * nta);
-                double* xs = sm;
-                gather_window(pred, tx, ty, tz, xs);
-                __syncthreads();
-                double* out = td.ypart + (size_t)tile * D3;
-                if (__ldg(td.tile_kind + tile) == TILE_FULL)
-                    full_tile(tx, ty, tz, xs, out);
-                else
-                    mixed_tile(tile, tx, ty, tz, xs, out);
-                __syncthreads();
-            }
+            const int tile = __ldg(td.item_list + item);
+            const int nta = td.nta;
+            if (!CUTCELL_OK_IF(tile < nta * nta * nta, 9, tile, (td.work + 64))) continue;
+            const int tx = tile % nta, ty = (tile / nta) % nta, tz = tile / (nta * nta);
+            double* xs = sm;
+            gather_window(pred, tx, ty, tz, xs);
+            __syncthreads();
+            if (item >= td.n_mixed)
+                full_tile(tx, ty, tz, xs, td.ypart + (size_t)tile * D3);
+            else
+                mixed_tile(tile, tx, ty, tz, xs, td.ypart + (size_t)tile * D3);
+            __syncthreads();
         }
-        // cut elements, one per warp, claimed warp by warp
+        // warp-level items: cut elements, then (if warp-level) full tiles
         const int lane = threadIdx.x & 31;
-        double* xe = sm + (size_t)(threadIdx.x >> 5) * Pa;
+        double* ws = sm + (size_t)(threadIdx.x >> 5) * WS;
+        const int n_warp_items = td.n_cut + (td.full_warp ? td.n_items - td.n_mixed : 0);
         while (true) {
-            int c = 0;
-            if (lane == 0) c = (int)atomicAdd(td.work2, 1u);
-            c = __shfl_sync(0xffffffffu, c, 0);
-            if (c >= td.n_cut) break;
-            cut_element_warp(pred, c, xe);
+            int w = 0;
+            if (lane == 0) w = (int)atomicAdd(td.work2, 1u);
+            w = __shfl_sync(0xffffffffu, w, 0);
+            if (w >= n_warp_items) break;
+            if (w < td.n_cut)
+                cut_element_warp(pred, w, ws);
+            else
+                full_tile_warp(pred, __ldg(td.item_list + td.n_mixed + (w - td.n_cut)), ws);
         }
         __syncthreads();
+    }
+
+    // full-space value of DOF i by one thread: its (up to 8) tile partials
+    // and its cut-element partials, summed in a fixed order.
+    __device__ __forceinline__ double yfull1(int i) const {
+        const int nb = td.nb, nta = td.nta;
+        const int ix = i % nb, iy = (i / nb) % nb, iz = i / (nb * nb);
+        const int t1x = min(ix / T, nta - 1), t1y = min(iy / T, nta - 1), t1z = min(iz / T, nta - 1);
+        double s = 0.0;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int tz = t1z - ((m >> 2) & 1), ty = t1y - ((m >> 1) & 1), tx = t1x - (m & 1);
+            if (tz < 0 || ty < 0 || tx < 0) continue;
+            if (iz - tz * T >= D || iy - ty * T >= D || ix - tx * T >= D) continue;
+            const int tile = (tz * nta + ty) * nta + tx;
+            s += __ldcg(td.ypart + (size_t)tile * D3 + ((iz - tz * T) * D + (iy - ty * T)) * D + (ix - tx * T));
+        }
+        const int slot = __ldg(td.cut_dof_slot + i);
+        if (slot >= 0) {
+            const int k1 = __ldg(td.cut_dof_ptr + slot + 1);
+            int k = __ldg(td.cut_dof_ptr + slot);
+            for (; k + 4 <= k1; k += 4) {  // four entries' loads in flight
+                int e[4];
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) e[u] = __ldg(td.cut_dof_ent + k + u);
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    v[u] = CUTCELL_OK_IF(e[u] >= 0 && e[u] < td.n_cut * P, 13, e[u], (td.work + 64)) ? __ldcg(td.ycut + e[u]) : 0.0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) s += v[u];
+            }
+            for (; k < k1; ++k) {
+                const int e = __ldg(td.cut_dof_ent + k);
+                if (CUTCELL_OK_IF(e >= 0 && e < td.n_cut * P, 13, e, (td.work + 64))) s += __ldcg(td.ycut + e);
+            }
+        }
+        return s;
     }
 
     // full-space value of DOF i, summed by the 4 lanes q = 0..3 of a group
@@ -468,38 +649,88 @@ struct TileOp {
 
     // phase 0: small-row values of E p; phase 1: tiles and cut elements;
     // phase 2a: full-space values of the DOFs the scatter reads; phase 2b:
-    // y = E^T yf and the partial of p.y.  Groups of 4 lanes own one DOF/row.
+    // y = E^T yf and the partial of p.y.  A DOF / row is owned by a group of 4
+    // lanes (small problems) or by one thread (large ones).
     __device__ __forceinline__ double apply(const double* p, double* y, const GridSync& gs, double* sm) const {
         td.ext.small_rows(p);
         if (!grid_sync(gs)) return 0.0;
+        return apply_tail(p, y, gs, sm);
+    }
+
+    // Phase 0 also forms p_new = D^-1 r + beta p_old for every reduced DOF
+    // (written to pnew), its small rows computed from the same formula.
+    __device__ __forceinline__ double apply_next(const double* pold, double* pnew, const double* r, const double* dinv,
+                                                 double beta, double* y, const GridSync& gs, double* sm) const {
+        const int n = td.ext.n_red;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            pnew[i] = p_next(__ldg(dinv + i), __ldcg(r + i), beta, __ldcg(pold + i));
+        td.ext.small_rows_next(pold, r, dinv, beta);
+        if (!grid_sync(gs)) return 0.0;
+        return apply_tail(pnew, y, gs, sm);
+    }
+
+    // phases 1-2b of the apply (phase 0 has completed grid-wide)
+    __device__ __forceinline__ double apply_tail(const double* p, double* y, const GridSync& gs, double* sm) const {
         phase1(p, sm);
         if (!grid_sync(gs)) return 0.0;
         if (blockIdx.x == 0 && threadIdx.x == 0) {  // every block has left phase 1
             *td.work = 0u;
             *td.work2 = 0u;
         }
-        const int q = threadIdx.x & 3;
-        const int g0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 2;
-        const int ng = (gridDim.x * blockDim.x) >> 2;
+        const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+        const int gstride = gridDim.x * blockDim.x;
         const int nneed = td.n_need;
-        for (int kb = g0 - (g0 & 7); kb < nneed; kb += ng) {  // warp-uniform trip count
-            const int k = kb + (g0 & 7);
-            const bool ok = k < nneed;
-            const int i = ok ? __ldg(td.need + k) : 0;
-            const double v = yfull4(i, q);
-            if (ok && q == 0) td.yfv[i] = v;
+        const int nred = td.ext.n_red;
+        if (!td.lane1) {  // few DOFs per thread: groups of 4 lanes split the long lists
+            const int q = threadIdx.x & 3;
+            const int g0 = gtid >> 2;
+            const int ng = gstride >> 2;
+            for (int kb = g0 - (g0 & 7); kb < nneed; kb += ng) {  // warp-uniform trip count
+                const int k = kb + (g0 & 7);
+                const bool ok = k < nneed;
+                const int i = ok ? __ldg(td.need + k) : 0;
+                const double v = yfull4(i, q);
+                if (ok && q == 0) td.yfv[i] = v;
+            }
+            if (!grid_sync(gs)) return 0.0;
+            double part = 0.0;
+            for (int jb = g0 - (g0 & 7); jb < nred; jb += ng) {
+                const int j = jb + (g0 & 7);
+                const bool ok = j < nred;
+                const double yj = scatter_row4(ok ? j : 0, q);
+                if (ok && q == 0) {
+                    y[j] = yj;
+                    part += __ldcg(p + j) * yj;
+                }
+            }
+            return part;
+        }
+        for (int k = gtid; k < nneed; k += gstride) {
+            const int i = __ldg(td.need + k);
+            td.yfv[i] = yfull1(i);
         }
         if (!grid_sync(gs)) return 0.0;
         double part = 0.0;
-        const int nred = td.ext.n_red;
-        for (int jb = g0 - (g0 & 7); jb < nred; jb += ng) {
-            const int j = jb + (g0 & 7);
-            const bool ok = j < nred;
-            const double yj = scatter_row4(ok ? j : 0, q);
-            if (ok && q == 0) {
-                y[j] = yj;
-                part += __ldcg(p + j) * yj;
+        for (int j = gtid; j < nred; j += gstride) {
+            double yj = __ldcg(td.yfv + __ldg(td.ext.full_of_red + j));
+            const int k1 = __ldg(td.ext.smallT_ptr + j + 1);
+            int k = __ldg(td.ext.smallT_ptr + j);
+            for (; k + 4 <= k1; k += 4) {  // four entries' loads in flight
+                int rw[4];
+                double vv[4], yv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    rw[u] = __ldg(td.ext.smallT_row + k + u);
+                    vv[u] = __ldg(td.ext.smallT_val + k + u);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) yv[u] = __ldcg(td.yfv + rw[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) yj += vv[u] * yv[u];
             }
+            for (; k < k1; ++k) yj += __ldg(td.ext.smallT_val + k) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k));
+            y[j] = yj;
+            part += __ldcg(p + j) * yj;
         }
         return part;
     }

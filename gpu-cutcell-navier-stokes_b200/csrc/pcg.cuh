@@ -32,6 +32,7 @@ struct PcgBufs {
     double* p;
     double* Ap;
     double* part;        // [8][nblocks]
+    double* p2;          // second search-direction buffer (operators that fuse the p update)
 };
 
 // Inner PCG on A d = rhs from d = 0.  Returns the status; *iters receives the
@@ -68,8 +69,19 @@ __device__ int pcg_core(const Op& op, const PcgBufs& B, const double* rhs, doubl
     int status = CUTCELL_E_NOCONV;
     int k = 0;
     double rel = 1.0;
+    // Operators with kFusedP form p_k = D^-1 r + beta p_{k-1} inside the first
+    // phase of their apply (double-buffered p), which saves the grid barrier
+    // that a separate p update needs; the others update p here.
+    double* P[2] = {B.p, Op::kFusedP ? B.p2 : B.p};
+    double beta = 0.0;
     for (k = 1; k <= maxiter; ++k) {
-        double pap = op.apply(B.p, B.Ap, gs, sm);
+        double* pk = P[(k - 1) & 1];
+        double pap;
+        if constexpr (Op::kFusedP) {
+            pap = (k > 1) ? op.apply_next(P[k & 1], pk, B.r, B.dinv, beta, B.Ap, gs, sm) : op.apply(pk, B.Ap, gs, sm);
+        } else {
+            pap = op.apply(pk, B.Ap, gs, sm);
+        }
         if (grid_error(gs)) return CUTCELL_E_BARRIER;
         pap = block_sum(pap, sh);
         if (threadIdx.x == 0) part[2 * nb + blockIdx.x] = pap;
@@ -82,7 +94,7 @@ __device__ int pcg_core(const Op& op, const PcgBufs& B, const double* rhs, doubl
         const double alpha = rz / pap;
         double rr_p = 0.0, rzn_p = 0.0;
         for (int i = gtid; i < n; i += gstride) {
-            const double pi = B.p[i];
+            const double pi = __ldcg(pk + i);
             d[i] += alpha * pi;
             const double ri = B.r[i] - alpha * __ldcg(B.Ap + i);
             B.r[i] = ri;
@@ -111,10 +123,12 @@ __device__ int pcg_core(const Op& op, const PcgBufs& B, const double* rhs, doubl
             status = CUTCELL_E_NAN;
             break;
         }
-        const double beta = rzn / rz;
+        beta = rzn / rz;
         rz = rzn;
-        for (int i = gtid; i < n; i += gstride) B.p[i] = B.dinv[i] * B.r[i] + beta * B.p[i];
-        if (!grid_sync(gs)) return CUTCELL_E_BARRIER;
+        if constexpr (!Op::kFusedP) {
+            for (int i = gtid; i < n; i += gstride) B.p[i] = p_next(B.dinv[i], B.r[i], beta, B.p[i]);
+            if (!grid_sync(gs)) return CUTCELL_E_BARRIER;
+        }
     }
     *iters = (k > maxiter) ? maxiter : k;
     *rel_out = rel;

@@ -94,6 +94,7 @@ class CutcellTileDesc(C.Structure):
         ("smallT_row", _P),
         ("smallT_val", _P),
         ("diag", _P),
+        ("n_mixed", C.c_int32),
     ]
 
 

@@ -105,7 +105,19 @@ def build_extension(
     preserve_degree: int | None = None,
     mass_diag: np.ndarray | None = None,
     chunk: int = 64,
+    neighbour_search: str = "auto",
 ) -> Extension:
+    """Polynomial-preserving extension (code/bell_3d_core.py:471-542).
+
+    ``neighbour_search``: "dense" sorts all interior Greville distances per
+    small DOF with NumPy's default argsort, as the reference does (bit-exact
+    E, ties included).  "tree" takes the nearest candidates from a k-d tree
+    (everything at or inside the needed radius, sorted by distance with ties
+    in interior order): the same kind of polynomial-preserving extension,
+    but equidistant neighbours at the cut-off may be chosen differently from
+    the reference's unstable sort.  "auto" keeps the dense search up to
+    5e8 small x interior distances (n <= 40 at p = 3) and uses the tree
+    beyond, where the dense sort takes minutes."""
     deg = degree if preserve_degree is None else int(preserve_degree)
     gamma = np.asarray(gamma, dtype=float)
     active = np.where(gamma > 0.0)[0]
@@ -143,9 +155,36 @@ def build_extension(
     poly = monomial_rows_3d(basis, deg)
     n_terms = poly.shape[0]
     gi = greville[interior]
+    # only the first 6 n_terms + 8 neighbours are ever used (the rank loop below)
+    need = 6 * n_terms + 8
+    tree = None
+    use_tree = neighbour_search == "tree" or (
+        neighbour_search == "auto" and interior.size > 4 * need and small.size * interior.size > 5.0e8
+    )
+    if use_tree:
+        from scipy.spatial import cKDTree
+
+        tree = cKDTree(gi)
+
+    def nearest_order(blk):
+        """Per small DOF: interior positions by Greville distance, ties in
+        interior order (the stable order of a full argsort), at least the
+        first ``need`` of them."""
+        if tree is None:
+            return np.argsort(np.linalg.norm(gi[None, :, :] - greville[blk][:, None, :], axis=2), axis=1)
+        out = []
+        dk, _ = tree.query(greville[blk], k=need)
+        for r, b in enumerate(blk):
+            # every point at or inside the need-th distance, ties included
+            cand = np.asarray(tree.query_ball_point(greville[int(b)], r=float(dk[r, -1]) * (1.0 + 1e-9) + 1e-300))
+            cand.sort()
+            dist = np.linalg.norm(gi[cand] - greville[int(b)], axis=1)
+            out.append(cand[np.argsort(dist, kind="stable")])
+        return out
+
     for s0 in range(0, small.size, chunk):
         blk = small[s0 : s0 + chunk]
-        order = np.argsort(np.linalg.norm(gi[None, :, :] - greville[blk][:, None, :], axis=2), axis=1)
+        order = nearest_order(blk)
         for r, b in enumerate(blk):
             ordered = interior[order[r]]
             k = n_terms

@@ -46,6 +46,7 @@ class TileLayout:
     cut_dof_slot: np.ndarray  # (n_full,)
     cut_dof_ptr: np.ndarray
     cut_dof_ent: np.ndarray  # cut * P + local row
+    n_mixed: int = 0  # leading mixed tiles in item_list (block-level items; full tiles are warp-level)
 
     @property
     def tile_list(self) -> np.ndarray:
@@ -116,7 +117,8 @@ def build_tile_layout(prob: CutCellProblem, tile: int = 4, cut_chunk: int = 2) -
     else:
         ptr = np.zeros(1, dtype=np.int32)
         ent = np.zeros(0, dtype=np.int32)
-    return TileLayout(T, nta, kind, item_list, eptr, tile_elem, TM, TA, TK, cut_chunk, cut_base, slot, ptr, ent)
+    return TileLayout(T, nta, kind, item_list, eptr, tile_elem, TM, TA, TK, cut_chunk, cut_base, slot, ptr, ent,
+                      n_mixed=len(mixed))
 
 
 def jacobi_diagonal(prob: CutCellProblem, ext: Extension) -> np.ndarray:
@@ -234,6 +236,7 @@ class CutCellOperator:
         desc.tile = lay.tile
         desc.n_tiles_axis = lay.n_tiles_axis
         desc.n_items = int(lay.item_list.size)
+        desc.n_mixed = int(lay.n_mixed)
         desc.cut_chunk = int(lay.cut_chunk)
         desc.n_cut = int(prob.cut_ids.size)
         desc.n_full = prob.n_full

@@ -246,7 +246,10 @@ def build_problem(
                 xq[ex][:, None, None, :], xq[ey][:, None, :, None], xq[ez][:, :, None, None]
             )  # (m, qz, qy, qx)
             F = F * wq[ez][:, :, None, None] * wq[ey][:, None, :, None] * wq[ex][:, None, None, :]
-            vals = np.einsum("mcba,mck,mbj,mai->mkji", F, Nq[ez], Nq[ey], Nq[ex])
+            # one axis at a time (the four-operand einsum is a naive 7-deep loop)
+            t = np.einsum("mcba,mai->mcbi", F, Nq[ex])
+            t = np.einsum("mcbi,mbj->mcji", t, Nq[ey])
+            vals = np.einsum("mcji,mck->mkji", t, Nq[ez])
             np.add.at(load, rows_all[idx].ravel(), vals.reshape(-1))
     # box-face Dirichlet data on full boundary elements
     if nitsche and dirichlet is not None:

@@ -99,6 +99,7 @@ typedef struct {
     const int32_t* smallT_row;
     const double* smallT_val;
     const double* diag;        /* [n_red] diagonal of E^T A E (Jacobi) */
+    int32_t n_mixed;           /* leading mixed tiles in item_list (the rest are full tiles) */
 } CutcellTileDesc;
 
 /* Replaces the CuPy CSR upload + Jacobi-CG loop of solve_gpu_cg

@@ -221,3 +221,21 @@ def test_native_setup_matches_python(kind):
     np.testing.assert_allclose(b.load, a.load, rtol=0, atol=1e-13 * np.abs(a.load).max())
     np.testing.assert_allclose(b.gamma, a.gamma, rtol=0, atol=1e-13)
     np.testing.assert_allclose(b.cut_fractions, a.cut_fractions, rtol=0, atol=1e-14)
+
+
+def test_extension_tree_search_is_a_valid_extension():
+    """The k-d tree neighbour search (used for large grids) gives the same
+    index sets and identity rows as the reference-ordered search and a
+    polynomial-preserving E; only the choice among equidistant neighbours
+    at the cut-off may differ."""
+    from cutcell_b200.aggregation import build_extension
+    from cutcell_b200.workloads import sphere_poisson
+
+    prob, _ = sphere_poisson(16, 3, 0.31)
+    a = build_extension(prob.gamma, prob.basis, 3, neighbour_search="dense")
+    b = build_extension(prob.gamma, prob.basis, 3, neighbour_search="tree")
+    for f in ("interior", "small_support", "active"):
+        assert np.array_equal(getattr(a, f), getattr(b, f))
+    rows = a.interior
+    assert (a.E[rows] != b.E[rows]).nnz == 0
+    assert b.polynomial_residual < 1e-11
