@@ -114,6 +114,17 @@ class ClockSampler:
         }
 
 
+# DRAM bytes (read + write) per launch of each workload's dominant kernel, from
+# one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the same
+# command; None where no capture was made for that configuration.
+NCU_TRAFFIC = {
+    ("sphere", 32, 3): 643.6e6 + 26.2e6,   # pcg_kernel, one whole solve
+    ("apply", 64, 3): 266.6e6 + 8.1e6,     # apply_kernel, one apply
+    ("batch", 72): 17.6e6,                 # batch_pcg_kernel, one launch
+    ("hill-step",): 161.7e6 + 32.6e6,      # hill_segment_kernel, one 3-component advection
+}
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -309,8 +320,8 @@ def run_batch(args, rank, world, local):
                 "d2h_bytes_per_step": 8 * nvec},
         "gpu_launches": int(args.steps),
         "roofline": {"bound": "hbm", "kernel": "batch_pcg_kernel (whole batch, one launch)", "achieved": achieved,
-                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind, "traffic": None,
-                     "algorithmic_bytes": bytes_alg,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
+                     "traffic": NCU_TRAFFIC.get(("batch", args.batch_count)), "algorithmic_bytes": bytes_alg,
                      "note": "algorithmic bytes per iteration 12 nnz + 13*8 n; the CSR slices and vectors are held in shared memory"},
     }
     if rank == 0 and not args.no_cpu_baseline and world == 1:
@@ -516,6 +527,12 @@ def run_hill_step(args, rank, world, local):
                    "l2": "flushed between timed steps", "setup_s": setup_s, "advect_ms": ta,
                    "advect_gflops": flop_adv / (ta * 1e-3) / 1e9},
         "clocks": clocks, "gpu_launches": (3 * 4 + 3 + 15) * args.steps,
+        # the advection kernel is FP64-FMA bound (no tensor-core FP64 kind on this path);
+        # peak: B200 FP64 nominal, not measured on this pool
+        "roofline": {"bound": "fp64", "kernel": "hill_segment_kernel (one 3-component advection)",
+                     "achieved": flop_adv / (ta * 1e-3) / 1e12, "peak": 37.0, "unit": "TFLOP/s",
+                     "frac": flop_adv / (ta * 1e-3) / 1e12 / 37.0, "peak_kind": "nominal",
+                     "traffic": NCU_TRAFFIC.get(("hill-step",))},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -573,7 +590,8 @@ def run_apply(args, rank, world, local):
                    "setup_s": setup_s, "l2": "flushed between applies"},
         "variants": out,
         "roofline": {"bound": "hbm", "kernel": "apply_kernel<TileOp<double>>", "achieved": out["fp64"]["GBps"], "peak": hbm,
-                     "unit": "GB/s", "frac": out["fp64"]["frac"], "peak_kind": kind, "traffic": None},
+                     "unit": "GB/s", "frac": out["fp64"]["frac"], "peak_kind": kind,
+                     "traffic": NCU_TRAFFIC.get(("apply", args.n, args.p)), "algorithmic_bytes": out["fp64"]["bytes"]},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -749,7 +767,8 @@ def main():
             "unit": "GB/s",
             "frac": achieved / hbm,
             "peak_kind": hbm_kind,
-            "traffic": None,
+            "traffic": NCU_TRAFFIC.get(("sphere", args.n, args.p)),
+            "traffic_per": "launch (one solve)",
             "bytes_per_iter": bytes_iter,
         },
     }
