@@ -100,17 +100,21 @@ __device__ __forceinline__ double p_next(double dinv, double r, double beta, dou
 }
 
 template <typename T> struct Conv;
+// ld: read-only global load; sld: shared-memory load, both widened to acc
 template <> struct Conv<double> {
     typedef double acc;
     __device__ __forceinline__ static double ld(const double* p) { return __ldg(p); }
+    __device__ __forceinline__ static double sld(const double* p) { return *p; }
 };
 template <> struct Conv<float> {
     typedef float acc;
     __device__ __forceinline__ static float ld(const float* p) { return __ldg(p); }
+    __device__ __forceinline__ static float sld(const float* p) { return *p; }
 };
 template <> struct Conv<__nv_bfloat16> {
     typedef float acc;
     __device__ __forceinline__ static float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+    __device__ __forceinline__ static float sld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
 };
 
 // Optional self-checks (build with -DCUTCELL_DEBUG_CHECKS): a failed check

@@ -483,27 +483,81 @@ struct TileOp {
     // column c of the row-major block is row c: for fixed c the 32 lanes read
     // 32 consecutive entries), ceil(P/32) independent accumulators per lane.
     static constexpr int RPL = (P + 31) / 32;
+    // Dense cut-element block product by one warp.  When a column of the block
+    // is a whole number of 16-byte pieces (p = 3 in every storage type), the
+    // block is streamed through two shared-memory chunk buffers with 16-byte
+    // cp.async copies: the next chunk is in flight while the current one is
+    // multiplied, so each warp keeps about 10 KB of loads outstanding (the
+    // completion wait is cp.async.wait_group, a hardware wait).
     __device__ void cut_element_warp(const double* pred, int c, double* xe) const {
         typedef typename Conv<CT>::acc acc_t;
         const int lane = threadIdx.x & 31;
         const int nb = td.nb;
         const int base = __ldg(td.cut_base + c);
-        for (int k = lane; k < P; k += 32) {
-            const int a = k % P1, b = (k / P1) % P1, cc = k / PP;
-            xe[k] = td.ext.gather_fast(pred, base + (cc * nb + b) * nb + a);
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) {
+            const int k = lane + 32 * t;
+            if (k < P) {
+                const int a = k % P1, b = (k / P1) % P1, cc = k / PP;
+                xe[k] = td.ext.gather_fast(pred, base + (cc * nb + b) * nb + a);
+            }
         }
-        __syncwarp();
         const CT* A = cut_mats + (size_t)c * P * P;
         acc_t acc[RPL];
 #pragma unroll
         for (int q = 0; q < RPL; ++q) acc[q] = 0;
-#pragma unroll 8
-        for (int col = 0; col < P; ++col) {
-            const acc_t xv = (acc_t)xe[col];
-            const CT* Ac = A + (size_t)col * P + lane;
+        constexpr int COLB = P * (int)sizeof(CT);  // bytes per column
+        if constexpr (COLB % 16 == 0) {
+            constexpr int BUFB = ((WS - Pa) * 8 / 2) / COLB * COLB;  // bytes per chunk buffer
+            constexpr int CPC = BUFB / COLB;                         // columns per chunk
+            constexpr int NCH = (P + CPC - 1) / CPC;
+            static_assert(CPC >= 1, "chunk buffer holds no column");
+            char* bufs = reinterpret_cast<char*>(xe + Pa);
+            const char* src = reinterpret_cast<const char*>(A);
+            auto issue = [&](int ch) {
+                const int c0 = ch * CPC;
+                const int bytes = min(CPC, P - c0) * COLB;
+                char* dst = bufs + (ch & 1) * BUFB;
+                const char* s = src + (size_t)c0 * COLB;
+                for (int off = lane * 16; off < bytes; off += 32 * 16) {
+                    const unsigned d = (unsigned)__cvta_generic_to_shared(dst + off);
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(s + off) : "memory");
+                }
+                asm volatile("cp.async.commit_group;\n" ::: "memory");
+            };
+            issue(0);
+            __syncwarp();  // xe complete
+            for (int ch = 0; ch < NCH; ++ch) {
+                if (ch + 1 < NCH) {
+                    issue(ch + 1);
+                    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+                } else {
+                    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                }
+                __syncwarp();  // every lane's pieces of chunk ch have landed
+                const CT* As = reinterpret_cast<const CT*>(bufs + (ch & 1) * BUFB);
+                const int c0 = ch * CPC;
+#pragma unroll 2
+                for (int cl = 0; cl < CPC; ++cl) {
+                    if (c0 + cl < P) {
+                        const acc_t xv = (acc_t)xe[c0 + cl];
 #pragma unroll
-            for (int q = 0; q < RPL; ++q)
-                if (lane + 32 * q < P) acc[q] += Conv<CT>::ld(Ac + 32 * q) * xv;
+                        for (int q = 0; q < RPL; ++q)
+                            if (lane + 32 * q < P) acc[q] += Conv<CT>::sld(As + cl * P + lane + 32 * q) * xv;
+                    }
+                }
+                __syncwarp();  // chunk buffer (ch & 1) is refilled by issue(ch + 2)
+            }
+        } else {
+            __syncwarp();
+#pragma unroll 8
+            for (int col = 0; col < P; ++col) {
+                const acc_t xv = (acc_t)xe[col];
+                const CT* Ac = A + (size_t)col * P + lane;
+#pragma unroll
+                for (int q = 0; q < RPL; ++q)
+                    if (lane + 32 * q < P) acc[q] += Conv<CT>::ld(Ac + 32 * q) * xv;
+            }
         }
 #pragma unroll
         for (int q = 0; q < RPL; ++q)
