@@ -6,7 +6,7 @@
 // single-system kernel (pcg.cuh, pcg_core).
 //
 // Work decomposition
-//   * A team is one thread-block cluster of C CTAs (C = 1, 2, 4 or 8).  Teams
+//   * A team is one thread-block cluster of C CTAs (C = 1, 2, 4, 8 or 16).  Teams
 //     claim problems from a global counter in a host-chosen order (heaviest
 //     first), so uneven sizes balance without any grid-wide barrier.
 //   * A problem's rows are split into C contiguous slices, one per CTA.  Each
@@ -36,7 +36,7 @@ namespace cg = cooperative_groups;
 void cutcell_internal_set_error(const std::string& what);
 
 #define BATCH_MAX_THREADS 512
-#define BATCH_MAX_CLUSTER 8
+#define BATCH_MAX_CLUSTER 16  // 16 is a non-portable cluster size (allowed on B200)
 #define BATCH_MAX_N 16384  // per system: the full copy of p must sit in shared memory
 
 namespace {
@@ -94,7 +94,7 @@ struct BatchSmem {
         q = r + vec_bytes(rows_max);
         d = q + vec_bytes(rows_max);
         slots = d + vec_bytes(rows_max);
-        mat = slots + 8 * 5 * 3 * BATCH_MAX_CLUSTER;  // 5 reduction groups x 3 values x 8 ranks
+        mat = slots + 8 * 5 * 3 * BATCH_MAX_CLUSTER;  // 5 reduction groups x 3 values x 16 ranks
         total = mat + mat_bytes;
     }
 };
@@ -597,7 +597,8 @@ int cutcell_batch_configure(cutcell_batch* B, const CutcellBatchConfig* cfg, con
                             const int32_t* order) {
     if (!B || !cfg || !lanes_per_row || !order) return CUTCELL_E_ARG;
     const int C = cfg->cluster, T = cfg->threads;
-    if (!(C == 1 || C == 2 || C == 4 || C == 8)) return arg_error("batch: cluster must be 1, 2, 4 or 8");
+    if (!(C == 1 || C == 2 || C == 4 || C == 8 || C == 16))
+        return arg_error("batch: cluster must be 1, 2, 4, 8 or 16");
     if (T < 32 || T > BATCH_MAX_THREADS || (T % 32) != 0) return arg_error("batch: threads must be 32..512, x32");
     if (cfg->smem_matrix < 0 || (cfg->smem_matrix % 16) != 0)
         return arg_error("batch: smem_matrix must be a non-negative multiple of 16");
@@ -632,6 +633,7 @@ int cutcell_batch_configure(cutcell_batch* B, const CutcellBatchConfig* cfg, con
                              std::to_string(optin - static_bytes),
                          CUTCELL_E_SHAPE);
     BCK(cudaFuncSetAttribute(batch_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total));
+    if (C > 8) BCK(cudaFuncSetAttribute(batch_pcg_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
 
     cudaLaunchConfig_t lc;
     memset(&lc, 0, sizeof(lc));

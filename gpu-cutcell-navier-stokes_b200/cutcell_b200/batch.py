@@ -32,13 +32,13 @@ from .fast_solver_backends import SolverReport, _report_from, as_csr
 SMEM_OPTIN = 232448  # per-CTA opt-in shared memory on B200 (227 KB)
 SMEM_PER_SM = 233472  # per-SM shared memory (228 KB)
 _STATIC_SMEM = 512  # static shared memory of the kernel, rounded up
-_SLOTS = 8 * 5 * 3 * 8  # reduction slots
+_SLOTS = 8 * 5 * 3 * 16  # reduction slots (5 groups x 3 values x 16 ranks)
 _RESERVED_PER_CTA = 1024  # shared memory the runtime reserves per resident CTA
 
 
 @dataclass(frozen=True)
 class BatchConfig:
-    cluster: int = 1  # CTAs per team (thread-block cluster)
+    cluster: int = 1  # CTAs per team (thread-block cluster): 1, 2, 4, 8 or 16
     threads: int = 256  # threads per CTA
     staging: str = "full"  # "none": CSR read from global; "full": one CTA per SM; "half": two per SM
     nnz_per_lane: int = 8  # target nonzeros per lane of a row group
@@ -239,7 +239,7 @@ class BatchSolver:
         its = np.array([max(1, int(r.iterations)) for r in reports], dtype=float)
         self.costs = self.packed.nnz.astype(float) * its
 
-    def autotune(self, *, tol=1e-9, maxiter=5000, preconditioner="jacobi", reps: int = 2, clusters=(1, 2, 4, 8)):
+    def autotune(self, *, tol=1e-9, maxiter=5000, preconditioner="jacobi", reps: int = 2, clusters=(1, 2, 4, 8, 16)):
         """Coordinate search over (cluster, staging), then threads, then lanes
         per row, timing the real batch on the current device rhs (device time
         of the captured solve, best of ``reps``).  Keeps the fastest."""

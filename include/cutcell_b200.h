@@ -257,7 +257,7 @@ int cutcell_hill_destroy(cutcell_hill* hill);
  * are in the reports. */
 typedef struct cutcell_batch cutcell_batch;
 typedef struct {
-    int32_t cluster;      /* CTAs per team: 1, 2, 4 or 8 */
+    int32_t cluster;      /* CTAs per team: 1, 2, 4, 8 or 16 (16 is a non-portable cluster size) */
     int32_t threads;      /* threads per CTA: multiple of 32, <= 512 */
     int32_t smem_matrix;  /* bytes per CTA for a staged CSR slice (multiple of 16; 0 = never stage) */
     int32_t teams;        /* concurrent teams (0 = as many as fit, at most n_problems) */

@@ -64,7 +64,7 @@ def test_pack_and_split_round_trip():
 
 
 def test_staging_budgets_fit_shared_memory():
-    for c in (1, 2, 4, 8):
+    for c in (1, 2, 4, 8, 16):
         for mode in ("none", "half", "full"):
             cfg = bt.BatchConfig(cluster=c, staging=mode)
             m = bt.staging_bytes(cfg, 841)

@@ -73,7 +73,7 @@ def _check(results, systems, rhs, oracle=None):
         assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-6, i
 
 
-@pytest.mark.parametrize("cluster", [1, 2, 4, 8])
+@pytest.mark.parametrize("cluster", [1, 2, 4, 8, 16])
 @pytest.mark.parametrize("staging", ["none", "full"])
 def test_golden_systems_all_shapes(torch_cuda, golden_systems, cluster, staging):
     from cutcell_b200.batch import BatchConfig, solve_batch
