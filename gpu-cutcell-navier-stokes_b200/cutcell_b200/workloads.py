@@ -68,6 +68,39 @@ def sphere_poisson(n: int = 32, p: int = 3, radius: float = 0.31, a_mass: float 
     return prob, ext
 
 
+def cube_volume_below(normal, c: float) -> float:
+    """Volume of {x in [0,1]^3 : normal . x <= c} for a normal with positive
+    components (inclusion-exclusion over the cube's vertices)."""
+    nrm = np.asarray(normal, dtype=float)
+    s = 0.0
+    for vx in (0, 1):
+        for vy in (0, 1):
+            for vz in (0, 1):
+                t = c - (nrm[0] * vx + nrm[1] * vy + nrm[2] * vz)
+                if t > 0.0:
+                    s += (-1.0) ** (vx + vy + vz) * t**3
+    return s / (6.0 * nrm[0] * nrm[1] * nrm[2])
+
+
+def sliver_plane(n: int, normal, fraction: float) -> PlaneLevelSet:
+    """Plane ``normal . x >= c`` (normal on the positive octant) whose worst cut
+    cell -- the corner cell at the origin, which has the largest local offset --
+    keeps exactly ``fraction`` of its volume as fluid: bisection on the local
+    offset of that cell, then c = h * local offset."""
+    nrm = np.abs(np.asarray(normal, dtype=float))
+    nrm = nrm / np.linalg.norm(nrm)
+    if np.any(nrm <= 0.0):
+        raise ValueError("the normal must lie strictly inside the positive octant")
+    lo, hi = 0.0, float(nrm.sum())
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if 1.0 - cube_volume_below(nrm, mid) > fraction:
+            lo = mid
+        else:
+            hi = mid
+    return PlaneLevelSet(tuple(nrm), 0.5 * (lo + hi) / n)
+
+
 def plane_offset_for_fraction(n: int, angle_deg: float, fraction: float) -> float:
     """Offset of the plane n.x = c such that the smallest nonzero cut-cell
     fluid fraction equals ``fraction`` (bisection on the exact polyhedral

@@ -239,3 +239,20 @@ def test_extension_tree_search_is_a_valid_extension():
     rows = a.interior
     assert (a.E[rows] != b.E[rows]).nnz == 0
     assert b.polynomial_residual < 1e-11
+
+
+def test_sliver_plane_worst_fraction_and_cube_volume():
+    """Closed-form cube volume under a plane, and the sliver plane's worst
+    cut cell against the product's cut quadrature."""
+    from cutcell_b200.problem import build_problem
+    from cutcell_b200.workloads import cube_volume_below, sliver_plane
+
+    nrm = np.array([0.3, 0.5, 0.81])
+    nrm /= np.linalg.norm(nrm)
+    assert abs(cube_volume_below(nrm, nrm.sum())) - 1.0 < 1e-14 and cube_volume_below(nrm, 0.0) == 0.0
+    # midpoint symmetry: the plane through the centre halves the cube
+    assert abs(cube_volume_below(nrm, 0.5 * nrm.sum()) - 0.5) < 1e-14
+    for eps in (1e-4, 0.05):
+        phi = sliver_plane(8, [1.0, 2.0, 0.7], eps)
+        prob = build_problem(phi, 8, 3)
+        assert abs(prob.min_cut_fraction / eps - 1.0) < 1e-8
