@@ -152,6 +152,69 @@ def manufactured_sine():
     return u, f
 
 
+def manufactured_sine_grad():
+    """Gradient of u = sin(pi x) sin(pi y) sin(pi z)."""
+    k = np.pi
+
+    def g(x, y, z):
+        sx, sy, sz = np.sin(k * x), np.sin(k * y), np.sin(k * z)
+        cx, cy, cz = np.cos(k * x), np.cos(k * y), np.cos(k * z)
+        return k * cx * sy * sz, k * sx * cy * sz, k * sx * sy * cz
+
+    return g
+
+
+def solution_errors(prob: "CutCellProblem", phi, alpha, u, grad_u, q: int | None = None) -> dict:
+    """Relative L2, H1-seminorm and maximum errors of u_h = sum alpha_i B_i
+    against (u, grad u) over the fluid domain, as solve_poisson_3d reports
+    them (code/cut_3d_sbp.py:506-531): ||u_h - u|| / ||u||, ||grad(u_h - u)|| /
+    ||grad u||, max|u_h - u| / max|u| over the quadrature nodes.  Uncut
+    elements use a (p+3)^3 tensor Gauss rule, cut elements the cut-cell rule
+    of the given order (default 2p+2)."""
+    from .cutgeom import cut_cell_quadrature
+
+    p, n, nb = prob.degree, prob.n_elements, prob.n_basis
+    h = prob.basis.h
+    q = q or 2 * p + 2
+    A3 = np.asarray(alpha, dtype=float).reshape(nb, nb, nb)  # (z, y, x)
+    acc = {"e2": 0.0, "u2": 0.0, "g2": 0.0, "gu2": 0.0, "emax": 0.0, "umax": 0.0}
+
+    def add(pts, w, ex, ey, ez):
+        Nx, Dx = local_values(prob.basis, np.full(len(w), ex), pts[:, 0])
+        Ny, Dy = local_values(prob.basis, np.full(len(w), ey), pts[:, 1])
+        Nz, Dz = local_values(prob.basis, np.full(len(w), ez), pts[:, 2])
+        C = A3[ez : ez + p + 1, ey : ey + p + 1, ex : ex + p + 1]
+        uh = np.einsum("cba,mc,mb,ma->m", C, Nz, Ny, Nx)
+        gx = np.einsum("cba,mc,mb,ma->m", C, Nz, Ny, Dx)
+        gy = np.einsum("cba,mc,mb,ma->m", C, Nz, Dy, Nx)
+        gz = np.einsum("cba,mc,mb,ma->m", C, Dz, Ny, Nx)
+        ue = u(pts[:, 0], pts[:, 1], pts[:, 2])
+        ux, uy, uz = grad_u(pts[:, 0], pts[:, 1], pts[:, 2])
+        acc["e2"] += float(np.sum(w * (uh - ue) ** 2))
+        acc["u2"] += float(np.sum(w * ue**2))
+        acc["g2"] += float(np.sum(w * ((gx - ux) ** 2 + (gy - uy) ** 2 + (gz - uz) ** 2)))
+        acc["gu2"] += float(np.sum(w * (ux**2 + uy**2 + uz**2)))
+        acc["emax"] = max(acc["emax"], float(np.max(np.abs(uh - ue))))
+        acc["umax"] = max(acc["umax"], float(np.max(np.abs(ue))))
+
+    xg, wg = gauss_legendre01(p + 3)
+    Z, Y, X = np.meshgrid(xg, xg, xg, indexing="ij")
+    W3 = (wg[:, None, None] * wg[None, :, None] * wg[None, None, :]).ravel() * h**3
+    ref = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    for ez, ey, ex in zip(*np.nonzero(prob.elem_type == FULL)):
+        add((np.array([ex, ey, ez]) + ref) * h, W3, ex, ey, ez)
+    for lin in prob.cut_ids:
+        ez, ey, ex = int(lin) // (n * n), (int(lin) // n) % n, int(lin) % n
+        cq = cut_cell_quadrature(phi, np.array([ex, ey, ez]) * h, h, q, box_faces=False)
+        if cq.wv.size:
+            add(cq.xv, cq.wv, ex, ey, ez)
+    return {
+        "l2": np.sqrt(acc["e2"] / acc["u2"]),
+        "h1": np.sqrt(acc["g2"] / acc["gu2"]),
+        "linf": acc["emax"] / acc["umax"],
+    }
+
+
 def build_problem(
     phi,
     n_elements: int,
