@@ -211,3 +211,85 @@ def build_extension(
     for row in poly:
         res = max(res, float(np.max(np.abs(E @ row[interior] - row * active_mask))))
     return Extension(E, interior, small, active, gamma, res)
+
+
+# ---- 1D and tensor-product aggregation (axis-aligned cut boxes) ----
+
+
+def cut_interval_gamma(basis: OpenUniformBasis, left: float) -> np.ndarray:
+    """gamma_i = int_left^1 N_i^2 / int_0^1 N_i^2 on the cut interval [left, 1]
+    (the diagonal ratio of assemble_cut_matrices' H and H_background,
+    code/cut_spline_sbp.py:90-146), by Gauss rules exact for N_i^2."""
+    from .bspline import gauss_legendre01, local_values
+
+    p, ne, h = basis.degree, basis.n_elements, basis.h
+    xg, wg = gauss_legendre01(p + 1)
+    cut = np.zeros(basis.n_basis)
+    full = np.zeros(basis.n_basis)
+    for e in range(ne):
+        a, b = e * h, (e + 1) * h
+        for lo, acc in ((a, full), (max(a, left), cut)):
+            if b <= lo:
+                continue
+            x = lo + (b - lo) * xg
+            N, _ = local_values(basis, np.full(x.size, e), x)
+            acc[e : e + p + 1] += ((b - lo) * wg) @ (N * N)
+    g = np.zeros_like(cut)
+    pos = full > 0.0
+    g[pos] = cut[pos] / full[pos]
+    return g
+
+
+def extension_1d(basis: OpenUniformBasis, left: float, support_threshold: float = 0.05,
+                 preserve_degree: int | None = None, active_tol: float = 1.0e-25):
+    """polynomial_preserving_extension on the cut interval [left, 1]
+    (code/cut_spline_sbp.py:156-198): interior functions (gamma >= threshold)
+    get identity columns; each small active function takes the least-squares
+    weights that reproduce the monomials up to the degree from its nearest
+    interior Greville neighbours (ties in interior order), the stencil grown
+    from degree + 1 up to degree + 6 until the moment block has full rank.
+    Returns (E dense (n_basis, n_red), interior, small, active, gamma, degree)."""
+    from .bspline import polynomial_coefficients
+
+    gamma = cut_interval_gamma(basis, left)
+    active = np.where(gamma > active_tol)[0]
+    interior = np.where(gamma >= support_threshold)[0]
+    small = active[gamma[active] < support_threshold]
+    if interior.size == 0:
+        raise ValueError("no interior basis functions")
+    deg = min(basis.degree if preserve_degree is None else preserve_degree, interior.size - 1)
+    poly = polynomial_coefficients(basis, deg)
+    col = np.full(basis.n_basis, -1, dtype=np.int64)
+    col[interior] = np.arange(interior.size)
+    E = np.zeros((basis.n_basis, interior.size))
+    E[interior, np.arange(interior.size)] = 1.0
+    g = basis.greville
+    for i in small:
+        ordered = interior[np.argsort(np.abs(g[interior] - g[i]), kind="stable")]
+        chosen = ordered[: deg + 1]
+        for k in range(deg + 1, min(ordered.size, deg + 6) + 1):
+            if np.linalg.matrix_rank(poly[:, ordered[:k]], tol=1.0e-12) == deg + 1:
+                chosen = ordered[:k]
+                break
+        w = np.linalg.lstsq(poly[:, chosen], poly[:, i], rcond=None)[0]
+        E[i, col[chosen]] = w
+    return E, interior, small, active, gamma, deg
+
+
+def tensor_extension(basis: OpenUniformBasis, lefts, support_threshold: float = 0.05,
+                     preserve_degree: int | None = None) -> Extension:
+    """E = Ez (x) Ey (x) Ex of a cut box with low-side cuts at ``lefts``
+    (assemble_cut_3d, code/cut_3d_sbp.py:89-146).  Reduced columns follow the
+    Kronecker order (z slowest); DOFs are x-fastest."""
+    parts = [extension_1d(basis, float(a), support_threshold, preserve_degree) for a in lefts]
+    (Ex, ix, _, ax, gx, _), (Ey, iy, _, ay, gy, _), (Ez, iz, _, az, gz, _) = parts
+    E = sp.kron(sp.csr_matrix(Ez), sp.kron(sp.csr_matrix(Ey), sp.csr_matrix(Ex))).tocsr()
+    E.eliminate_zeros()
+    E.sort_indices()
+    nb = basis.n_basis
+    lin = lambda sz, sy, sx: ((sz[:, None, None] * nb + sy[None, :, None]) * nb + sx[None, None, :]).ravel()
+    interior = lin(iz, iy, ix)
+    active = np.sort(lin(az, ay, ax))
+    small = np.setdiff1d(active, interior)
+    gamma = np.kron(gz, np.kron(gy, gx))
+    return Extension(E, interior, small, active, gamma, 0.0)

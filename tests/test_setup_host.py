@@ -284,3 +284,30 @@ def test_plane_poisson_converges_at_optimal_order():
     assert np.log2(errs[0]["l2"] / errs[1]["l2"]) > 3.5  # p + 1 = 4
     assert np.log2(errs[0]["h1"] / errs[1]["h1"]) > 2.7  # p = 3
     assert errs[1]["l2"] < 1e-4 and errs[1]["h1"] < 1e-3
+
+
+def test_tensor_aggregation_matches_reference(golden):
+    """1D polynomial-preserving extension and the tensor E of a cut box
+    against the reference's own (tests/golden/tensor_ext.npz)."""
+    from cutcell_b200.aggregation import extension_1d, tensor_extension
+    from cutcell_b200.bspline import make_basis
+
+    z = np.load(golden / "tensor_ext.npz")
+    for k in range(int(z["count"])):
+        n, p, frac = z[f"c{k}_meta"]
+        b = make_basis(int(n), int(p))
+        E, interior, small, active, gamma, deg = extension_1d(b, b.h * frac)
+        np.testing.assert_array_equal(interior, z[f"c{k}_interior"])
+        np.testing.assert_allclose(gamma, z[f"c{k}_gamma"], rtol=1e-12, atol=1e-16)
+        assert E.shape == z[f"c{k}_E"].shape
+        assert np.abs(E - z[f"c{k}_E"]).max() < 1e-10
+    n, p = (int(v) for v in z["box_meta"][:2])
+    fr = z["box_meta"][2:]
+    b = make_basis(n, p)
+    ext = tensor_extension(b, [b.h * f for f in fr])
+    Eref = z["box_E"]
+    assert ext.E.shape == Eref.shape
+    assert np.abs(ext.E.toarray() - Eref).max() < 1e-10
+    # the device layout accepts it: identity rows are the interior DOFs
+    lay = ext.device_layout()
+    assert np.array_equal(lay["full_of_red"], ext.interior)
