@@ -63,9 +63,10 @@ struct HillAdvDev {
 // q0 + HILL_WARPS*r + w through (a)-(c); after a CTA barrier every warp adds
 // all the round's points into the modes it owns (a = w + HILL_WARPS t) in (d).
 // Dynamic shared memory: the segment's coefficient rows C[a][comp][iz]
-// (lmax x 3 x nz) and per warp two 9 x nz buffers.
+// (lmax x 3 x nz), per warp two 9 x nz buffers, and the z tables (basis
+// values, derivatives, weights of every z element, laid out lane-contiguous).
 template <int LMAX>
-__global__ void __launch_bounds__(HILL_WARPS * 32) hill_segment_kernel(HillAdvDev d, const double* ux,
+__global__ void __launch_bounds__(HILL_WARPS * 32, 4) hill_segment_kernel(HillAdvDev d, const double* ux,
                                                                       const double* uy, const double* uz,
                                                                       double* part) {
     constexpr int LW = (LMAX + HILL_WARPS - 1) / HILL_WARPS;  // modes owned per warp
@@ -77,6 +78,17 @@ __global__ void __launch_bounds__(HILL_WARPS * 32) hill_segment_kernel(HillAdvDe
     double* Tw = Cs + LMAX * 3 * nz + w * 18 * nz;
     double* PXYall = Cs + LMAX * 3 * nz + 9 * nz;  // warp w' buffer at PXYall + w' * 18 nz
     double* PXY = PXYall + w * 18 * nz;
+    // z tables, lane-contiguous: V[(k * NZB + j) * nz + e], wz[k * nz + e]
+    const int qpe = d.qpe;
+    double* zV = Cs + LMAX * 3 * nz + HILL_WARPS * 18 * nz;
+    double* zD = zV + qpe * HILL_NZB * nz;
+    double* zW = zD + qpe * HILL_NZB * nz;
+    for (int e = threadIdx.x; e < nz * qpe * HILL_NZB; e += blockDim.x) {
+        const int el_ = e / (qpe * HILL_NZB), k = (e / HILL_NZB) % qpe, j = e % HILL_NZB;
+        zV[(k * HILL_NZB + j) * nz + el_] = __ldg(d.Vl + e);
+        zD[(k * HILL_NZB + j) * nz + el_] = __ldg(d.dVl + e);
+    }
+    for (int e = threadIdx.x; e < nz * qpe; e += blockDim.x) zW[(e % qpe) * nz + e / qpe] = __ldg(d.wzl + e);
     const int L = d.seg_len[s];
     const int* pat = d.pat_idx + d.seg_pat[s];
     const double* U[3] = {ux, uy, uz};
@@ -142,15 +154,14 @@ __global__ void __launch_bounds__(HILL_WARPS * 32) hill_segment_kernel(HillAdvDe
                     double Pl[HILL_NZB], Xl[HILL_NZB], Yl[HILL_NZB];
 #pragma unroll
                     for (int j = 0; j < HILL_NZB; ++j) Pl[j] = Xl[j] = Yl[j] = 0.0;
-                    for (int k = 0; k < d.qpe; ++k) {
-                        const int o = (lane * d.qpe + k) * HILL_NZB;
+                    for (int k = 0; k < qpe; ++k) {
                         double vl[HILL_NZB], dvl[HILL_NZB];
 #pragma unroll
                         for (int j = 0; j < HILL_NZB; ++j) {
-                            vl[j] = __ldg(d.Vl + o + j);
-                            dvl[j] = __ldg(d.dVl + o + j);
+                            vl[j] = zV[(k * HILL_NZB + j) * nz + lane];
+                            dvl[j] = zD[(k * HILL_NZB + j) * nz + lane];
                         }
-                        const double wk = __ldg(d.wzl + lane * d.qpe + k);
+                        const double wk = zW[k * nz + lane];
                         double u[3] = {0.0, 0.0, 0.0};
                         double gx = 0.0, gy = 0.0, gz = 0.0;
 #pragma unroll
@@ -445,7 +456,8 @@ int cutcell_hill_create(const CutcellHillDesc* desc, cutcell_hill** out) {
     d.M2inv = h.M2inv;
     H->n_part = h.n_part;
     const int lm = h.lmax <= 16 ? 16 : (h.lmax <= 24 ? 24 : 32);
-    H->smem = sizeof(double) * ((size_t)lm * 3 * h.nz + (size_t)HILL_WARPS * 18 * h.nz);
+    H->smem = sizeof(double) * ((size_t)lm * 3 * h.nz + (size_t)HILL_WARPS * 18 * h.nz +
+                                (size_t)h.nz * h.qpe * (2 * HILL_NZB + 1));
     const size_t fld = (size_t)h.nr * h.nz;
     cudaError_t e = cudaGetDevice(&H->device);
     if (e == cudaSuccess) e = cudaMalloc(&H->part, sizeof(double) * (size_t)h.n_part * 3 * h.nz);
