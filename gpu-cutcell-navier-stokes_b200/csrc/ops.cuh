@@ -204,7 +204,7 @@ struct TileOp {
     // pass buffers, or a cut element's gathered values
     static constexpr int WS = (4 * D3a > Pa) ? 4 * D3a : Pa;
     static size_t smem_bytes() {
-        const size_t mixed = (size_t)D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa + 3 * 4 * 2 * PP;
+        const size_t mixed = (size_t)D3a + (size_t)2 * NW * D3a + (size_t)2 * NW * 4 * Pa + 3 * 4 * 2 * PP;
         const size_t full = 5 * (size_t)D3a;
         const size_t warp = (size_t)NW * WS;
         size_t m = mixed > warp ? mixed : warp;
@@ -397,14 +397,19 @@ struct TileOp {
         __syncwarp();
     }
 
+    // Uncut elements of a mixed tile, one per half-warp (16 lanes), so a block
+    // has 2 NW elements in flight; each half-warp accumulates into its own
+    // window, summed in a fixed order at the end.
+    static constexpr int NH = 2 * NW;  // half-warps per block
     __device__ void mixed_tile(int tile, int tx, int ty, int tz, double* xs, double* out) const {
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        double* acc = xs + D3a + (size_t)warp * D3a;
-        double* e0 = xs + D3a + (size_t)NW * D3a + (size_t)warp * 4 * Pa;
+        const int half = threadIdx.x >> 4, hl = threadIdx.x & 15;
+        const unsigned hmask = 0xffffu << (16 * ((threadIdx.x >> 4) & 1));
+        double* acc = xs + D3a + (size_t)half * D3a;
+        double* e0 = xs + D3a + (size_t)NH * D3a + (size_t)half * 4 * Pa;
         double* e1 = e0 + Pa;
         double* e2 = e1 + Pa;
         double* e3 = e2 + Pa;
-        double* fac = xs + D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa;  // [axis][4 pos][M, K~][PP]
+        double* fac = xs + D3a + (size_t)NH * D3a + (size_t)NH * 4 * Pa;  // [axis][4 pos][M, K~][PP]
         const int n = td.n;
         for (int k = threadIdx.x; k < 3 * 4 * 2 * PP; k += blockDim.x) {
             const int e = k % PP, w = (k / PP) % 2, pos = (k / (2 * PP)) % 4, ax = k / (8 * PP);
@@ -414,10 +419,10 @@ struct TileOp {
             if (ax == 0 && w == 1) v += td.a_mass * __ldg(td.M1 + (size_t)el * PP + e);  // a M + K~ on x
             fac[k] = v;
         }
-        for (int k = lane; k < D3; k += 32) acc[k] = 0.0;
+        for (int k = hl; k < D3; k += 16) acc[k] = 0.0;
         __syncthreads();
         const int eb = __ldg(td.tile_eptr + tile), ee = __ldg(td.tile_eptr + tile + 1);
-        for (int it = eb + warp; it < ee; it += NW) {
+        for (int it = eb + half; it < ee; it += NH) {
             const int le = __ldg(td.tile_elem + it);
             const int lx = le % T, ly = (le / T) % T, lz = le / (T * T);
             const double* Mx = fac + ((0 * 4 + lx) * 2 + 0) * PP;
@@ -426,13 +431,13 @@ struct TileOp {
             const double* Ky = fac + ((1 * 4 + ly) * 2 + 1) * PP;
             const double* Mz = fac + ((2 * 4 + lz) * 2 + 0) * PP;
             const double* Kz = fac + ((2 * 4 + lz) * 2 + 1) * PP;
-            __syncwarp();
-            for (int k = lane; k < P; k += 32) {
+            __syncwarp(hmask);
+            for (int k = hl; k < P; k += 16) {
                 const int a = k % P1, b = (k / P1) % P1, c = k / PP;
                 e0[k] = xs[((lz + c) * D + (ly + b)) * D + (lx + a)];
             }
-            __syncwarp();
-            for (int k = lane; k < P; k += 32) {
+            __syncwarp(hmask);
+            for (int k = hl; k < P; k += 16) {
                 const int i = k % P1, row = k - i;
                 double s1 = 0.0, s2 = 0.0;
 #pragma unroll
@@ -443,8 +448,8 @@ struct TileOp {
                 e1[k] = s1;
                 e2[k] = s2;
             }
-            __syncwarp();
-            for (int k = lane; k < P; k += 32) {
+            __syncwarp(hmask);
+            for (int k = hl; k < P; k += 16) {
                 const int x = k % P1, i = (k / P1) % P1, z = k / PP;
                 double s1 = 0.0, s2 = 0.0;
 #pragma unroll
@@ -456,8 +461,8 @@ struct TileOp {
                 e3[k] = s1;
                 e0[k] = s2;
             }
-            __syncwarp();
-            for (int k = lane; k < P; k += 32) {
+            __syncwarp(hmask);
+            for (int k = hl; k < P; k += 16) {
                 const int xy = k % PP, i = k / PP;
                 double s = 0.0;
 #pragma unroll
@@ -473,7 +478,7 @@ struct TileOp {
         for (int k = threadIdx.x; k < D3; k += blockDim.x) {
             double s = 0.0;
 #pragma unroll
-            for (int w = 0; w < NW; ++w) s += acc0[(size_t)w * D3a + k];
+            for (int w = 0; w < NH; ++w) s += acc0[(size_t)w * D3a + k];
             out[k] = s;
         }
     }
