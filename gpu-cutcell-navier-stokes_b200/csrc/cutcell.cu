@@ -1,5 +1,6 @@
 // C ABI of libcutcell_b200.so: contexts, cooperative launches, status codes.
 // The persistent kernels live in pcg.cuh / ops.cuh.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -56,6 +57,16 @@ __global__ void to_f32_kernel(size_t n, const double* in, float* out) {
 __global__ void to_bf16_kernel(size_t n, const double* in, __nv_bfloat16* out) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         out[i] = __float2bfloat16((float)in[i]);
+}
+
+// Dense symmetric 64 x 64 cut blocks -> the 2080-entry split storage of
+// sym64_index (upper triangle, row <= column, of each row-major block).
+__global__ void pack_sym64_kernel(int n_cut, const double* dense, double* packed) {
+    const size_t n = (size_t)n_cut * 64 * 64;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int e = (int)(k / 4096), i = (int)((k / 64) % 64), j = (int)(k % 64);
+        if (i <= j) packed[(size_t)e * SYM64_ENTRIES + sym64_index(i, j)] = dense[k];
+    }
 }
 
 __global__ void ext_gather_kernel(ExtDev e, const double* xr, double* xf) {
@@ -131,12 +142,15 @@ struct cutcell_ctx {
     // tiles
     TileData td;
     const double* cut64 = nullptr;
+    double* cutsym = nullptr;  // degree 3: owned split-storage copy of the cut blocks
     float* cut32 = nullptr;
     __nv_bfloat16* cut16 = nullptr;
     double* ypart = nullptr;
     double* ycut = nullptr;
     double* yfv = nullptr;
     double* psmall = nullptr;
+    int4* need_rec = nullptr;
+    int4* row_rec = nullptr;
     // scratch
     double* dinv = nullptr;
     double* ones = nullptr;
@@ -369,6 +383,73 @@ int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const 
     return CUTCELL_OK;
 }
 
+// Phase-2 work records, built once on the host from the descriptor's lists:
+//   need_rec[k] = {full DOF i, 0, first, end of i's cut partials in cut_dof_ent}
+//   row_rec[k]  = {reduced row j, full DOF of j, first, end of j's E^T entries}
+// ordered by list length in buckets of 4 entries, longest first (index order
+// within a bucket).  Long lists then meet at the front, where the one-thread
+// form hands the lists longer than kHeavyList entries to groups of 4 lanes.
+// Also validates every index the phase-2 loops follow.
+constexpr int kHeavyList = 12;
+
+static int build_phase2(cutcell_ctx* c, const CutcellTileDesc* t) {
+    const int nneed = t->n_need, nred = t->n_red, nfull = (int)t->n_full;
+    std::vector<int> need(nneed), slot(nfull), fred(nred), tptr((size_t)nred + 1);
+    CK(cudaMemcpy(need.data(), t->need, sizeof(int) * nneed, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(slot.data(), t->cut_dof_slot, sizeof(int) * nfull, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(fred.data(), t->full_of_red, sizeof(int) * nred, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(tptr.data(), t->smallT_ptr, sizeof(int) * (nred + 1), cudaMemcpyDeviceToHost));
+    int nslots = 0;
+    for (int s : slot) nslots = std::max(nslots, s + 1);
+    std::vector<int> cptr((size_t)nslots + 1, 0);
+    CK(cudaMemcpy(cptr.data(), t->cut_dof_ptr, sizeof(int) * (nslots + 1), cudaMemcpyDeviceToHost));
+    // every cut partial index must lie in ycut ([n_cut][(p+1)^3])
+    const int P1 = t->degree + 1;
+    const long ncp = (long)t->n_cut * P1 * P1 * P1;
+    const int nent = cptr[nslots];
+    if (cptr[0] != 0 || nent < 0) return CUTCELL_E_SHAPE;
+    std::vector<int> ent((size_t)nent);
+    if (nent) CK(cudaMemcpy(ent.data(), t->cut_dof_ent, sizeof(int) * nent, cudaMemcpyDeviceToHost));
+    for (int e : ent)
+        if (e < 0 || e >= ncp) return CUTCELL_E_SHAPE;
+    std::vector<int4> nr(nneed), rr(nred);
+    for (int k = 0; k < nneed; ++k) {
+        const int i = need[k];
+        if (i < 0 || i >= nfull) return CUTCELL_E_SHAPE;
+        const int s = slot[i];
+        const int b = s >= 0 ? cptr[s] : 0, e = s >= 0 ? cptr[s + 1] : 0;
+        if (b < 0 || e < b || e > nent) return CUTCELL_E_SHAPE;
+        nr[k] = make_int4(i, 0, b, e);
+    }
+    if (tptr[0] != 0) return CUTCELL_E_SHAPE;
+    for (int j = 0; j < nred; ++j) {
+        if (fred[j] < 0 || fred[j] >= nfull || tptr[j + 1] < tptr[j]) return CUTCELL_E_SHAPE;
+        rr[j] = make_int4(j, fred[j], tptr[j], tptr[j + 1]);
+    }
+    std::vector<int> trow((size_t)tptr[nred]);
+    if (!trow.empty())
+        CK(cudaMemcpy(trow.data(), t->smallT_row, sizeof(int) * trow.size(), cudaMemcpyDeviceToHost));
+    for (int i : trow)
+        if (i < 0 || i >= nfull) return CUTCELL_E_SHAPE;
+    auto order = [](std::vector<int4>& v) {
+        std::stable_sort(v.begin(), v.end(), [](const int4& a, const int4& b) {
+            return (a.w - a.z) / 4 > (b.w - b.z) / 4;
+        });
+        int heavy = 0;
+        while (heavy < (int)v.size() && v[heavy].w - v[heavy].z > kHeavyList) ++heavy;
+        return heavy;
+    };
+    c->td.n_need_heavy = order(nr);
+    c->td.n_row_heavy = order(rr);
+    CK(cudaMalloc(&c->need_rec, sizeof(int4) * std::max(nneed, 1)));
+    CK(cudaMalloc(&c->row_rec, sizeof(int4) * std::max(nred, 1)));
+    if (nneed) CK(cudaMemcpy(c->need_rec, nr.data(), sizeof(int4) * nneed, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->row_rec, rr.data(), sizeof(int4) * nred, cudaMemcpyHostToDevice));
+    c->td.need_rec = c->need_rec;
+    c->td.row_rec = c->row_rec;
+    return CUTCELL_OK;
+}
+
 int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     if (!out || !t) return CUTCELL_E_ARG;
     const int p = t->degree, P1 = p + 1, P = P1 * P1 * P1, D = t->tile + p;
@@ -394,12 +475,22 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     CK(cudaMalloc(&c->yfv, (size_t)t->n_full * sizeof(double)));
     CK(cudaMalloc(&c->psmall, ((size_t)t->n_small + 1) * sizeof(double)));
     CK(cudaMemset(c->yfv, 0, (size_t)t->n_full * sizeof(double)));
-    const size_t ncm = (size_t)t->n_cut * P * P;
+    // degree 3 keeps its (symmetric) cut blocks in the split storage of
+    // sym64_index, half the bytes of the dense blocks; other degrees read the
+    // caller's dense blocks
+    c->cut64 = t->cut_mats;
+    size_t ncm = (size_t)t->n_cut * P * P;
+    if (p == 3 && t->n_cut > 0) {
+        ncm = (size_t)t->n_cut * SYM64_ENTRIES;
+        CK(cudaMalloc(&c->cutsym, ncm * sizeof(double)));
+        pack_sym64_kernel<<<592, 256>>>(t->n_cut, t->cut_mats, c->cutsym);
+        c->cut64 = c->cutsym;
+    }
     if (ncm) {
         CK(cudaMalloc(&c->cut32, ncm * sizeof(float)));
         CK(cudaMalloc(&c->cut16, ncm * sizeof(__nv_bfloat16)));
-        to_f32_kernel<<<592, 256>>>(ncm, t->cut_mats, c->cut32);
-        to_bf16_kernel<<<592, 256>>>(ncm, t->cut_mats, c->cut16);
+        to_f32_kernel<<<592, 256>>>(ncm, c->cut64, c->cut32);
+        to_bf16_kernel<<<592, 256>>>(ncm, c->cut64, c->cut16);
     }
     ExtDev e;
     e.n_full = t->n_full;
@@ -424,10 +515,11 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     d.n_items = t->n_items;
     d.n_mixed = t->n_mixed;
     {
-        // warp-level full tiles pay off once there are many per SM
+        // warp-level full tiles: always where their passes run on the FP64
+        // tensor cores (window D <= 8), else once there are many per SM
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-        d.full_warp = (t->n_items - t->n_mixed) >= 8 * (sms > 0 ? sms : 148) ? 1 : 0;
+        d.full_warp = (D <= 8 || (t->n_items - t->n_mixed) >= 8 * (sms > 0 ? sms : 148)) ? 1 : 0;
         // one thread per DOF once there are more than about two per thread of a 2 x 256 x SMs grid
         d.lane1 = t->n_need > 2 * 512 * (sms > 0 ? sms : 148) ? 1 : 0;
     }
@@ -456,7 +548,11 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     d.n_need = t->n_need;
     d.work = c->bar + 64;
     d.work2 = c->bar + 96;
-    c->cut64 = t->cut_mats;
+    st = build_phase2(c, t);
+    if (st) {
+        cutcell_destroy(c);
+        return st;
+    }
     diag_inv_kernel<<<ceil_div(t->n_red, 256), 256>>>(t->n_red, t->diag, c->dinv);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
@@ -569,7 +665,7 @@ int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
-    void* bufs[] = {c->val32, c->val16, c->cut32, c->cut16, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
                     c->p,     c->p2,    c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);

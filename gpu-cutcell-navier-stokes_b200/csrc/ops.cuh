@@ -180,9 +180,35 @@ struct TileData {
     double* yfv;               // [n_full] full-space values of the needed DOFs
     const int* need;           // [n_need] full DOFs read by the E^T scatter
     int n_need;
+    // phase-2 records, longest lists first (built by the host at create):
+    const int4* need_rec;      // [n_need] {full DOF, 0, cut partials [z, w) in cut_dof_ent}
+    const int4* row_rec;       // [n_red] {reduced row, its full DOF, E^T entries [z, w)}
+    int n_need_heavy;          // leading records whose lists are long (4 lanes each when lane1)
+    int n_row_heavy;
     unsigned* work;            // dynamic tile-item counter (reset in phase 2)
     unsigned* work2;           // dynamic cut-element counter, claimed per warp
 };
+
+// Storage of the symmetric 64 x 64 cut-element blocks of degree 3 (2080
+// entries, half of the dense block): with A split into 32 x 32 blocks
+// [[A00, A01], [A01^T, A11]],
+//   [0, 528)      A00 upper triangle, entry (a, b), a <= b, at b(b+1)/2 + a
+//   [528, 1040)   A01 columns 0..15 \ entry (a, c) of A01 at
+//   [1040, 1552)  A01 columns 16..31 / (c & 15) * 32 + ((a + c) & 31)
+//   [1552, 2080)  A11 upper triangle, packed like A00.
+// Triangular numbers b(b+1)/2 are distinct modulo 32 for b < 32, and the
+// (a + c) & 31 rotation spreads both a row and a column of A01 over all
+// banks, so every shared-memory walk below is (nearly) conflict free.  Every
+// chunk start and the element stride are multiples of 16 bytes in 8-, 4- and
+// 2-byte storage.
+constexpr int SYM64_ENTRIES = 2080;
+__host__ __device__ constexpr int sym64_index(int i, int j) {
+    const int a = i < j ? i : j, b = i < j ? j : i;
+    if (b < 32) return b * (b + 1) / 2 + a;
+    if (a >= 32) return 1552 + (b - 32) * (b - 31) / 2 + (a - 32);
+    const int c = b - 32;
+    return 528 + (c >> 4) * 512 + (c & 15) * 32 + ((a + c) & 31);
+}
 
 template <typename CT, int P1>
 struct TileOp {
@@ -197,6 +223,9 @@ struct TileOp {
     static constexpr int D3a = (D3 + 1) & ~1;
     static constexpr int Pa = (P + 1) & ~1;
     static constexpr int CTRL = 2;  // doubles reserved for the work-item slot
+    // degree 3 stores its cut blocks in the symmetric split layout above
+    static constexpr bool kSym = (P1 == 4);
+    static constexpr int CUT_ENTRIES = kSym ? SYM64_ENTRIES : P * P;
     TileData td;
     const CT* __restrict__ cut_mats;
 
@@ -284,11 +313,140 @@ struct TileOp {
         }
     }
 
+    // d += a b on the FP64 tensor cores (mma.sync m8n8k4, A 8x4 row-major, B
+    // 4x8 column-major).  Fragments of lane = 4 g + t: A(g, t), B(t, g),
+    // C(g, 2t) and C(g, 2t + 1).
+    __device__ __forceinline__ static void dmma(double& d0, double& d1, double a, double b) {
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                     : "+d"(d0), "+d"(d1)
+                     : "d"(a), "d"(b));
+    }
+
+    // The three banded passes of a full tile (window in xs, result to out) as
+    // batched 1D products on the FP64 tensor cores, for D <= 8.  Each pass is
+    // a (D^2 lines x D) by (D x D) product, lines in blocks of 8 (A), the 1D
+    // factor transposed in B (its D x D block padded to 8 x 8 with zeros, held
+    // in registers), the k dimension in ceil(D/4) steps:
+    //   x: u1 = X Mx^T, u2 = X Ax^T            (line = (z, y), k = x)
+    //   y: v1 = U1 My^T, v2 = U2 My^T + U1 Ky^T (line = (z, x), k = y)
+    //   z: out = V2 Mz^T + V1 Kz^T               (line = (y, x), k = z)
+    static constexpr int KS = (D + 3) / 4;
+    static constexpr int NLB = (D * D + 7) / 8;
+    __device__ void full_tile_passes_mma(int tx, int ty, int tz, int tile, double* ws) const {
+        static_assert(D <= 8, "tensor-core passes need D <= 8");
+        const int lane = threadIdx.x & 31;
+        const int g = lane >> 2, t4 = lane & 3;
+        const int nta = td.nta;
+        double* xs = ws;
+        double* u1 = ws + D3a;
+        double* u2 = u1 + D3a;
+        double* v2 = u2 + D3a;
+        double* v1 = xs;  // the window is dead after the x pass
+        // B fragments: B(k = j, n = i) = F[i][j]
+        auto bfrag = [&](const double* F, int ks) {
+            const int i = g, j = 4 * ks + t4;
+            return (i < D && j < D) ? __ldg(F + i * D + j) : 0.0;
+        };
+        double bMx[KS], bAx[KS], bMy[KS], bKy[KS], bMz[KS], bKz[KS];
+        {
+            const double* Mx = td.TM + (size_t)tx * D * D;
+            const double* Ax = td.TA + (size_t)tx * D * D;
+            const double* My = td.TM + (size_t)ty * D * D;
+            const double* Ky = td.TK + ((size_t)1 * nta + ty) * D * D;
+            const double* Mz = td.TM + (size_t)tz * D * D;
+            const double* Kz = td.TK + ((size_t)2 * nta + tz) * D * D;
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks) {
+                bMx[ks] = bfrag(Mx, ks);
+                bAx[ks] = bfrag(Ax, ks);
+                bMy[ks] = bfrag(My, ks);
+                bKy[ks] = bfrag(Ky, ks);
+                bMz[ks] = bfrag(Mz, ks);
+                bKz[ks] = bfrag(Kz, ks);
+            }
+        }
+        constexpr int L = D * D;
+        const int c0 = 2 * t4;  // this lane's two output columns c0, c0 + 1
+        // x pass: A(line, j) = xs[line * D + j]
+#pragma unroll 1
+        for (int mb = 0; mb < NLB; ++mb) {
+            const int line = 8 * mb + g;
+            double p0 = 0.0, p1 = 0.0, q0 = 0.0, q1 = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks) {
+                const int j = 4 * ks + t4;
+                const double a = (line < L && j < D) ? xs[line * D + j] : 0.0;
+                dmma(p0, p1, a, bMx[ks]);
+                dmma(q0, q1, a, bAx[ks]);
+            }
+            if (line < L) {
+                if (c0 < D) {
+                    u1[line * D + c0] = p0;
+                    u2[line * D + c0] = q0;
+                }
+                if (c0 + 1 < D) {
+                    u1[line * D + c0 + 1] = p1;
+                    u2[line * D + c0 + 1] = q1;
+                }
+            }
+        }
+        __syncwarp();
+        // y pass: line = (z, x), A(line, j) = U[(z * D + j) * D + x]
+#pragma unroll 1
+        for (int mb = 0; mb < NLB; ++mb) {
+            const int line = 8 * mb + g;
+            const int z = line / D, x = line - z * D;
+            double p0 = 0.0, p1 = 0.0, q0 = 0.0, q1 = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks) {
+                const int j = 4 * ks + t4;
+                const bool ok = line < L && j < D;
+                const double a1 = ok ? u1[(z * D + j) * D + x] : 0.0;
+                const double a2 = ok ? u2[(z * D + j) * D + x] : 0.0;
+                dmma(p0, p1, a1, bMy[ks]);
+                dmma(q0, q1, a2, bMy[ks]);
+                dmma(q0, q1, a1, bKy[ks]);
+            }
+            if (line < L) {
+                if (c0 < D) {
+                    v1[(z * D + c0) * D + x] = p0;
+                    v2[(z * D + c0) * D + x] = q0;
+                }
+                if (c0 + 1 < D) {
+                    v1[(z * D + c0 + 1) * D + x] = p1;
+                    v2[(z * D + c0 + 1) * D + x] = q1;
+                }
+            }
+        }
+        __syncwarp();
+        // z pass: line = (y, x), A(line, j) = V[j * D * D + line]
+        double* out = td.ypart + (size_t)tile * D3;
+#pragma unroll 1
+        for (int mb = 0; mb < NLB; ++mb) {
+            const int line = 8 * mb + g;
+            double p0 = 0.0, p1 = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks) {
+                const int j = 4 * ks + t4;
+                const bool ok = line < L && j < D;
+                const double a2 = ok ? v2[j * L + line] : 0.0;
+                const double a1 = ok ? v1[j * L + line] : 0.0;
+                dmma(p0, p1, a2, bMz[ks]);
+                dmma(p0, p1, a1, bKz[ks]);
+            }
+            if (line < L) {
+                if (c0 < D) out[c0 * L + line] = p0;
+                if (c0 + 1 < D) out[(c0 + 1) * L + line] = p1;
+            }
+        }
+        __syncwarp();
+    }
+
     // A full tile by one warp: E-gather of the D^3 window, then the x, y, z
     // banded passes with __syncwarp between them (no block barrier), so a
-    // block has NW tiles in flight.  Every per-lane loop has a compile-time
-    // trip count (KPL entries) and is unrolled, so a lane's loads are all in
-    // flight together instead of one entry's latency after another.
+    // block has NW tiles in flight: on the FP64 tensor cores for D <= 8, else
+    // per lane, where every loop has a compile-time trip count (KPL entries)
+    // and is unrolled, so a lane's loads are all in flight together.
     // ws: 4 * D3a doubles.
     static constexpr int KPL = (D3 + 31) / 32;
     __device__ void full_tile_warp(const double* pred, int tile, double* ws) const {
@@ -328,6 +486,10 @@ struct TileOp {
                 if (lane + 32 * t < D3) xs[lane + 32 * t] = xv[t];
         }
         __syncwarp();
+        if constexpr (D <= 8) {
+            full_tile_passes_mma(tx, ty, tz, tile, ws);
+            return;
+        }
         const double* Mx = td.TM + (size_t)tx * D * D;
         const double* Ax = td.TA + (size_t)tx * D * D;
         const double* My = td.TM + (size_t)ty * D * D;
@@ -507,12 +669,73 @@ struct TileOp {
                 xe[k] = td.ext.gather_fast(pred, base + (cc * nb + b) * nb + a);
             }
         }
-        const CT* A = cut_mats + (size_t)c * P * P;
+        const CT* A = cut_mats + (size_t)c * CUT_ENTRIES;
         acc_t acc[RPL];
 #pragma unroll
         for (int q = 0; q < RPL; ++q) acc[q] = 0;
         constexpr int COLB = P * (int)sizeof(CT);  // bytes per column
-        if constexpr (COLB % 16 == 0) {
+        if constexpr (kSym) {
+            // four chunks (A00, A01 left, A01 right, A11) through two buffers;
+            // lane l owns rows l (acc[0]) and 32 + l (acc[1]) and adds every
+            // row's terms in ascending column order, as the dense product does
+            constexpr int SLOT = 528 * (int)sizeof(CT);  // bytes per buffer (largest chunk)
+            static_assert(Pa + 2 * 528 * (int)sizeof(CT) / 8 <= WS, "chunk buffers exceed the warp slice");
+            char* bufs = reinterpret_cast<char*>(xe + Pa);
+            const char* src = reinterpret_cast<const char*>(A);
+            auto issue = [&](int ch) {
+                const int e0 = ch == 0 ? 0 : (ch == 1 ? 528 : (ch == 2 ? 1040 : 1552));
+                const int bytes = (ch == 0 || ch == 3 ? 528 : 512) * (int)sizeof(CT);
+                char* dst = bufs + (ch & 1) * SLOT;
+                const char* s = src + (size_t)e0 * sizeof(CT);
+                for (int off = lane * 16; off < bytes; off += 32 * 16) {
+                    const unsigned d = (unsigned)__cvta_generic_to_shared(dst + off);
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(s + off) : "memory");
+                }
+                asm volatile("cp.async.commit_group;\n" ::: "memory");
+            };
+            const int tl = lane * (lane + 1) / 2;
+            issue(0);
+            __syncwarp();  // xe complete
+#pragma unroll 1
+            for (int ch = 0; ch < 4; ++ch) {
+                if (ch + 1 < 4) {
+                    issue(ch + 1);
+                    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+                } else {
+                    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                }
+                __syncwarp();  // every lane's pieces of chunk ch have landed
+                const CT* S = reinterpret_cast<const CT*>(bufs + (ch & 1) * SLOT);
+                if (ch == 0 || ch == 3) {  // diagonal block: the whole row of lane l
+                    const int q = ch == 0 ? 0 : 1;
+                    const double* xs = xe + 32 * q;
+                    int tc = 0;
+#pragma unroll 8
+                    for (int cc = 0; cc < 32; ++cc) {
+                        const int a = cc >= lane ? tc + lane : tl + cc;
+                        acc[q] += Conv<CT>::sld(S + a) * (acc_t)xs[cc];
+                        tc += cc + 1;
+                    }
+                } else {
+                    const int cb = (ch - 1) * 16;  // first A01 column of this chunk
+                    // row walk: row l of A01, columns cb .. cb + 15 (global 32 + c)
+#pragma unroll 8
+                    for (int cc = 0; cc < 16; ++cc) {
+                        const int cg = cb + cc;
+                        acc[0] += Conv<CT>::sld(S + cc * 32 + ((lane + cg) & 31)) * (acc_t)xe[32 + cg];
+                    }
+                    // column walk: lanes whose A01 column lies in this chunk form
+                    // (A01^T x_0)_l, which precedes A11 in row 32 + l
+                    if ((lane >> 4) == ch - 1) {
+                        const int cl = lane & 15;
+#pragma unroll 8
+                        for (int r = 0; r < 32; ++r)
+                            acc[1] += Conv<CT>::sld(S + cl * 32 + ((r + lane) & 31)) * (acc_t)xe[r];
+                    }
+                }
+                __syncwarp();  // buffer (ch & 1) is refilled by issue(ch + 2)
+            }
+        } else if constexpr (COLB % 16 == 0) {
             constexpr int BUFB = ((WS - Pa) * 8 / 2) / COLB * COLB;  // bytes per chunk buffer
             constexpr int CPC = BUFB / COLB;                         // columns per chunk
             constexpr int NCH = (P + CPC - 1) / CPC;
@@ -629,87 +852,80 @@ struct TileOp {
         __syncthreads();
     }
 
-    // full-space value of DOF i by one thread: its (up to 8) tile partials
-    // and its cut-element partials, summed in a fixed order.
-    __device__ __forceinline__ double yfull1(int i) const {
+    // full-space value of DOF rec.x: its (up to 8) tile partials and its cut
+    // partials [rec.z, rec.w), summed by G = 1 thread or by the q-th of a
+    // group of G = 4 lanes (partials interleaved over the lanes, then a fixed
+    // xor tree, so every lane of the group returns the same bits).
+    template <int G>
+    __device__ __forceinline__ double yfull_rec(const int4 rec, int q) const {
+        const int i = rec.x;
         const int nb = td.nb, nta = td.nta;
         const int ix = i % nb, iy = (i / nb) % nb, iz = i / (nb * nb);
         const int t1x = min(ix / T, nta - 1), t1y = min(iy / T, nta - 1), t1z = min(iz / T, nta - 1);
         double s = 0.0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
+        for (int m = q; m < 8; m += G) {
             const int tz = t1z - ((m >> 2) & 1), ty = t1y - ((m >> 1) & 1), tx = t1x - (m & 1);
             if (tz < 0 || ty < 0 || tx < 0) continue;
             if (iz - tz * T >= D || iy - ty * T >= D || ix - tx * T >= D) continue;
             const int tile = (tz * nta + ty) * nta + tx;
             s += __ldcg(td.ypart + (size_t)tile * D3 + ((iz - tz * T) * D + (iy - ty * T)) * D + (ix - tx * T));
         }
-        const int slot = __ldg(td.cut_dof_slot + i);
-        if (slot >= 0) {
-            const int k1 = __ldg(td.cut_dof_ptr + slot + 1);
-            int k = __ldg(td.cut_dof_ptr + slot);
-            for (; k + 4 <= k1; k += 4) {  // four entries' loads in flight
+        int k = rec.z + q;
+        if constexpr (G == 1) {
+            for (; k + 4 <= rec.w; k += 4) {  // four entries' loads in flight
                 int e[4];
                 double v[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) e[u] = __ldg(td.cut_dof_ent + k + u);
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    v[u] = CUTCELL_OK_IF(e[u] >= 0 && e[u] < td.n_cut * P, 13, e[u], (td.work + 64)) ? __ldcg(td.ycut + e[u]) : 0.0;
+                for (int u = 0; u < 4; ++u) v[u] = __ldcg(td.ycut + e[u]);
 #pragma unroll
                 for (int u = 0; u < 4; ++u) s += v[u];
             }
-            for (; k < k1; ++k) {
-                const int e = __ldg(td.cut_dof_ent + k);
-                if (CUTCELL_OK_IF(e >= 0 && e < td.n_cut * P, 13, e, (td.work + 64))) s += __ldcg(td.ycut + e);
-            }
+        }
+        for (; k < rec.w; k += G) s += __ldcg(td.ycut + __ldg(td.cut_dof_ent + k));
+        if constexpr (G == 4) {
+            s += __shfl_xor_sync(0xffffffffu, s, 1);
+            s += __shfl_xor_sync(0xffffffffu, s, 2);
         }
         return s;
     }
 
-    // full-space value of DOF i, summed by the 4 lanes q = 0..3 of a group
-    // (tile partials and cut-element partials interleaved over the lanes,
-    // then a fixed xor tree): every lane returns the same bits.
-    __device__ __forceinline__ double yfull4(int i, int q) const {
-        const int nb = td.nb, nta = td.nta;
-        const int ix = i % nb, iy = (i / nb) % nb, iz = i / (nb * nb);
-        const int t1x = min(ix / T, nta - 1), t1y = min(iy / T, nta - 1), t1z = min(iz / T, nta - 1);
-        double s = 0.0;
-        // candidate tiles: 8 combinations, lane q takes combinations q and q+4
-        for (int m = q; m < 8; m += 4) {
-            const int tz = t1z - ((m >> 2) & 1), ty = t1y - ((m >> 1) & 1), tx = t1x - (m & 1);
-            if (tz < 0 || ty < 0 || tx < 0) continue;
-            if (iz - tz * T >= D || iy - ty * T >= D || ix - tx * T >= D) continue;
-            const int tile = (tz * nta + ty) * nta + tx;
-            s += __ldcg(td.ypart + (size_t)tile * D3 + ((iz - tz * T) * D + (iy - ty * T)) * D + (ix - tx * T));
-        }
-        const int slot = __ldg(td.cut_dof_slot + i);
-        if (slot >= 0) {
-            const int k1 = __ldg(td.cut_dof_ptr + slot + 1);
-            for (int k = __ldg(td.cut_dof_ptr + slot) + q; k < k1; k += 4) {
-                const int e = __ldg(td.cut_dof_ent + k);
-                if (CUTCELL_OK_IF(e >= 0 && e < td.n_cut * P, 13, e, (td.work + 64))) s += __ldcg(td.ycut + e);
+    // (E^T yf) of row rec.x: the value of its own DOF rec.y and its E^T
+    // entries [rec.z, rec.w), by G = 1 thread or a group of G = 4 lanes.
+    template <int G>
+    __device__ __forceinline__ double scatter_rec(const int4 rec, int q) const {
+        double y = (q == 0) ? __ldcg(td.yfv + rec.y) : 0.0;
+        int k = rec.z + q;
+        if constexpr (G == 1) {
+            for (; k + 4 <= rec.w; k += 4) {  // four entries' loads in flight
+                int rw[4];
+                double vv[4], yv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    rw[u] = __ldg(td.ext.smallT_row + k + u);
+                    vv[u] = __ldg(td.ext.smallT_val + k + u);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) yv[u] = __ldcg(td.yfv + rw[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) y += vv[u] * yv[u];
             }
         }
-        s += __shfl_xor_sync(0xffffffffu, s, 1);
-        s += __shfl_xor_sync(0xffffffffu, s, 2);
-        return s;
-    }
-
-    __device__ __forceinline__ double scatter_row4(int j, int q) const {
-        double y = (q == 0) ? __ldcg(td.yfv + __ldg(td.ext.full_of_red + j)) : 0.0;
-        const int k1 = __ldg(td.ext.smallT_ptr + j + 1);
-        for (int k = __ldg(td.ext.smallT_ptr + j) + q; k < k1; k += 4)
-            y += __ldg(td.ext.smallT_val + k) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k));
-        y += __shfl_xor_sync(0xffffffffu, y, 1);
-        y += __shfl_xor_sync(0xffffffffu, y, 2);
+        for (; k < rec.w; k += G) y += __ldg(td.ext.smallT_val + k) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k));
+        if constexpr (G == 4) {
+            y += __shfl_xor_sync(0xffffffffu, y, 1);
+            y += __shfl_xor_sync(0xffffffffu, y, 2);
+        }
         return y;
     }
 
     // phase 0: small-row values of E p; phase 1: tiles and cut elements;
     // phase 2a: full-space values of the DOFs the scatter reads; phase 2b:
-    // y = E^T yf and the partial of p.y.  A DOF / row is owned by a group of 4
-    // lanes (small problems) or by one thread (large ones).
+    // y = E^T yf and the partial of p.y.  Phase 2 walks the host-built
+    // records (longest lists first): each DOF / row is owned by a group of 4
+    // lanes (small problems, and the long lists of large ones) or by one thread.
     __device__ __forceinline__ double apply(const double* p, double* y, const GridSync& gs, double* sm) const {
         td.ext.small_rows(p);
         if (!grid_sync(gs)) return 0.0;
@@ -740,56 +956,44 @@ struct TileOp {
         const int gstride = gridDim.x * blockDim.x;
         const int nneed = td.n_need;
         const int nred = td.ext.n_red;
-        if (!td.lane1) {  // few DOFs per thread: groups of 4 lanes split the long lists
-            const int q = threadIdx.x & 3;
-            const int g0 = gtid >> 2;
-            const int ng = gstride >> 2;
-            for (int kb = g0 - (g0 & 7); kb < nneed; kb += ng) {  // warp-uniform trip count
+        // records [0, n4) by groups of 4 lanes (all of them when there are few
+        // per thread, else only the long lists), the rest one per thread
+        const int q = threadIdx.x & 3;
+        const int g0 = gtid >> 2;
+        const int ng = gstride >> 2;
+        const int4 none = make_int4(0, 0, 0, 0);
+        {
+            const int n4 = td.lane1 ? td.n_need_heavy : nneed;
+            for (int kb = g0 - (g0 & 7); kb < n4; kb += ng) {  // warp-uniform trip count
                 const int k = kb + (g0 & 7);
-                const bool ok = k < nneed;
-                const int i = ok ? __ldg(td.need + k) : 0;
-                const double v = yfull4(i, q);
-                if (ok && q == 0) td.yfv[i] = v;
+                const bool ok = k < n4;
+                const int4 rec = ok ? __ldg(td.need_rec + k) : none;
+                const double v = yfull_rec<4>(rec, q);
+                if (ok && q == 0) td.yfv[rec.x] = v;
             }
-            if (!grid_sync(gs)) return 0.0;
-            double part = 0.0;
-            for (int jb = g0 - (g0 & 7); jb < nred; jb += ng) {
-                const int j = jb + (g0 & 7);
-                const bool ok = j < nred;
-                const double yj = scatter_row4(ok ? j : 0, q);
-                if (ok && q == 0) {
-                    y[j] = yj;
-                    part += __ldcg(p + j) * yj;
-                }
+            for (int k = n4 + gtid; k < nneed; k += gstride) {
+                const int4 rec = __ldg(td.need_rec + k);
+                td.yfv[rec.x] = yfull_rec<1>(rec, 0);
             }
-            return part;
-        }
-        for (int k = gtid; k < nneed; k += gstride) {
-            const int i = __ldg(td.need + k);
-            td.yfv[i] = yfull1(i);
         }
         if (!grid_sync(gs)) return 0.0;
         double part = 0.0;
-        for (int j = gtid; j < nred; j += gstride) {
-            double yj = __ldcg(td.yfv + __ldg(td.ext.full_of_red + j));
-            const int k1 = __ldg(td.ext.smallT_ptr + j + 1);
-            int k = __ldg(td.ext.smallT_ptr + j);
-            for (; k + 4 <= k1; k += 4) {  // four entries' loads in flight
-                int rw[4];
-                double vv[4], yv[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    rw[u] = __ldg(td.ext.smallT_row + k + u);
-                    vv[u] = __ldg(td.ext.smallT_val + k + u);
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) yv[u] = __ldcg(td.yfv + rw[u]);
-#pragma unroll
-                for (int u = 0; u < 4; ++u) yj += vv[u] * yv[u];
+        const int n4 = td.lane1 ? td.n_row_heavy : nred;
+        for (int jb = g0 - (g0 & 7); jb < n4; jb += ng) {
+            const int k = jb + (g0 & 7);
+            const bool ok = k < n4;
+            const int4 rec = ok ? __ldg(td.row_rec + k) : none;
+            const double yj = scatter_rec<4>(rec, q);
+            if (ok && q == 0) {
+                y[rec.x] = yj;
+                part += __ldcg(p + rec.x) * yj;
             }
-            for (; k < k1; ++k) yj += __ldg(td.ext.smallT_val + k) * __ldcg(td.yfv + __ldg(td.ext.smallT_row + k));
-            y[j] = yj;
-            part += __ldcg(p + j) * yj;
+        }
+        for (int k = n4 + gtid; k < nred; k += gstride) {
+            const int4 rec = __ldg(td.row_rec + k);
+            const double yj = scatter_rec<1>(rec, 0);
+            y[rec.x] = yj;
+            part += __ldcg(p + rec.x) * yj;
         }
         return part;
     }

@@ -83,7 +83,9 @@ typedef struct {
     const double* TM;          /* [n_tiles_axis][D^2], D = tile+degree */
     const double* TA;          /* [n_tiles_axis][D^2] */
     const double* TK;          /* [3][n_tiles_axis][D^2] */
-    const double* cut_mats;    /* [n_cut][(p+1)^6] */
+    const double* cut_mats;    /* [n_cut][(p+1)^6] symmetric, row-major; degree 3 copies the
+                                  upper triangles (row <= column) into a half-size split
+                                  storage at create and reads only that afterwards */
     const int32_t* cut_base;   /* [n_cut] full index of each cut element's first DOF */
     const int32_t* cut_dof_slot; /* [n_full] slot in the DOF -> cut-element list, -1 if none */
     const int32_t* cut_dof_ptr;  /* [n_slots + 1] */
