@@ -386,17 +386,20 @@ int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const 
 // Phase-2 work records, built once on the host from the descriptor's lists:
 //   need_rec[k] = {full DOF i, 0, first, end of i's cut partials in cut_dof_ent}
 //   row_rec[k]  = {reduced row j, full DOF of j, first, end of j's E^T entries}
-// ordered by list length in buckets of 4 entries, longest first (index order
-// within a bucket).  Long lists then meet at the front, where the one-thread
-// form hands the lists longer than kHeavyList entries to groups of 4 lanes.
-// Also validates every index the phase-2 loops follow.
+// The records with a list come first, by list length in buckets of 4 entries,
+// longest first; the records without one (plain tile-partial sums and
+// identity rows, most of them) follow in index order, so neighbouring lanes
+// read neighbouring partials.  Lists longer than kHeavyList entries go to
+// groups of 4 lanes even where the rest runs one per thread.  Also validates
+// every index the phase-2 loops follow.
 constexpr int kHeavyList = 12;
 
 static int build_phase2(cutcell_ctx* c, const CutcellTileDesc* t) {
     const int nneed = t->n_need, nred = t->n_red, nfull = (int)t->n_full;
-    std::vector<int> need(nneed), slot(nfull), fred(nred), tptr((size_t)nred + 1);
+    std::vector<int> need(nneed), slot(nfull), rof(nfull), fred(nred), tptr((size_t)nred + 1);
     CK(cudaMemcpy(need.data(), t->need, sizeof(int) * nneed, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(slot.data(), t->cut_dof_slot, sizeof(int) * nfull, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(rof.data(), t->red_of_full, sizeof(int) * nfull, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(fred.data(), t->full_of_red, sizeof(int) * nred, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(tptr.data(), t->smallT_ptr, sizeof(int) * (nred + 1), cudaMemcpyDeviceToHost));
     int nslots = 0;
@@ -408,39 +411,43 @@ static int build_phase2(cutcell_ctx* c, const CutcellTileDesc* t) {
     const long ncp = (long)t->n_cut * P1 * P1 * P1;
     const int nent = cptr[nslots];
     if (cptr[0] != 0 || nent < 0) return CUTCELL_E_SHAPE;
+    for (int s = 0; s < nslots; ++s)
+        if (cptr[s + 1] < cptr[s]) return CUTCELL_E_SHAPE;
     std::vector<int> ent((size_t)nent);
     if (nent) CK(cudaMemcpy(ent.data(), t->cut_dof_ent, sizeof(int) * nent, cudaMemcpyDeviceToHost));
     for (int e : ent)
         if (e < 0 || e >= ncp) return CUTCELL_E_SHAPE;
     std::vector<int4> nr(nneed), rr(nred);
+    std::vector<char> needed((size_t)nfull, 0);
     for (int k = 0; k < nneed; ++k) {
         const int i = need[k];
         if (i < 0 || i >= nfull) return CUTCELL_E_SHAPE;
         const int s = slot[i];
-        const int b = s >= 0 ? cptr[s] : 0, e = s >= 0 ? cptr[s + 1] : 0;
-        if (b < 0 || e < b || e > nent) return CUTCELL_E_SHAPE;
-        nr[k] = make_int4(i, 0, b, e);
+        nr[k] = s >= 0 ? make_int4(i, 0, cptr[s], cptr[s + 1]) : make_int4(i, 0, 0, 0);
+        needed[i] = 1;
     }
     if (tptr[0] != 0) return CUTCELL_E_SHAPE;
     for (int j = 0; j < nred; ++j) {
-        if (fred[j] < 0 || fred[j] >= nfull || tptr[j + 1] < tptr[j]) return CUTCELL_E_SHAPE;
-        rr[j] = make_int4(j, fred[j], tptr[j], tptr[j + 1]);
+        const int f = fred[j];
+        if (f < 0 || f >= nfull || rof[f] != j || !needed[f] || tptr[j + 1] < tptr[j]) return CUTCELL_E_SHAPE;
+        rr[j] = make_int4(j, f, tptr[j], tptr[j + 1]);
     }
+    // the E^T lists may only read needed DOFs
     std::vector<int> trow((size_t)tptr[nred]);
     if (!trow.empty())
         CK(cudaMemcpy(trow.data(), t->smallT_row, sizeof(int) * trow.size(), cudaMemcpyDeviceToHost));
     for (int i : trow)
-        if (i < 0 || i >= nfull) return CUTCELL_E_SHAPE;
-    auto order = [](std::vector<int4>& v) {
-        std::stable_sort(v.begin(), v.end(), [](const int4& a, const int4& b) {
-            return (a.w - a.z) / 4 > (b.w - b.z) / 4;
-        });
-        int heavy = 0;
-        while (heavy < (int)v.size() && v[heavy].w - v[heavy].z > kHeavyList) ++heavy;
-        return heavy;
+        if (i < 0 || i >= nfull || !needed[i]) return CUTCELL_E_SHAPE;
+    auto order = [](std::vector<int4>& v, int* heavy, int* listed) {
+        auto key = [](const int4& a) { return a.w > a.z ? 1 + (a.w - a.z) / 4 : 0; };
+        std::stable_sort(v.begin(), v.end(), [&](const int4& a, const int4& b) { return key(a) > key(b); });
+        *heavy = 0;
+        while (*heavy < (int)v.size() && v[*heavy].w - v[*heavy].z > kHeavyList) ++*heavy;
+        *listed = *heavy;
+        while (*listed < (int)v.size() && v[*listed].w > v[*listed].z) ++*listed;
     };
-    c->td.n_need_heavy = order(nr);
-    c->td.n_row_heavy = order(rr);
+    order(nr, &c->td.n_need_heavy, &c->td.n_need_list);
+    order(rr, &c->td.n_row_heavy, &c->td.n_row_list);
     CK(cudaMalloc(&c->need_rec, sizeof(int4) * std::max(nneed, 1)));
     CK(cudaMalloc(&c->row_rec, sizeof(int4) * std::max(nred, 1)));
     if (nneed) CK(cudaMemcpy(c->need_rec, nr.data(), sizeof(int4) * nneed, cudaMemcpyHostToDevice));

@@ -180,11 +180,14 @@ struct TileData {
     double* yfv;               // [n_full] full-space values of the needed DOFs
     const int* need;           // [n_need] full DOFs read by the E^T scatter
     int n_need;
-    // phase-2 records, longest lists first (built by the host at create):
+    // phase-2 records (built by the host at create): those with a list first,
+    // longest first, then those without, in index order
     const int4* need_rec;      // [n_need] {full DOF, 0, cut partials [z, w) in cut_dof_ent}
     const int4* row_rec;       // [n_red] {reduced row, its full DOF, E^T entries [z, w)}
     int n_need_heavy;          // leading records whose lists are long (4 lanes each when lane1)
     int n_row_heavy;
+    int n_need_list;           // leading records with a non-empty list
+    int n_row_list;
     unsigned* work;            // dynamic tile-item counter (reset in phase 2)
     unsigned* work2;           // dynamic cut-element counter, claimed per warp
 };
@@ -559,11 +562,110 @@ struct TileOp {
         __syncwarp();
     }
 
+    // Uncut elements of a mixed tile for p = 3, one element per warp on the
+    // FP64 tensor cores (the element's 4-point lines fill k = 4 exactly), so
+    // a block has NW elements in flight.  Each pass is one or two m8n8k4
+    // products per 8 lines, the two factors a pass needs side by side in the
+    // n dimension:
+    //   x: [u1 | u2] = X [Mx^T | Ax^T]                 (line = (z, y))
+    //   y: [e3 | e0] = U1 [My^T | Ky^T] + U2 [0 | My^T] (line = (z, x))
+    //   z: s = E0 Mz^T + E3 Kz^T                        (line = (y, x))
+    // Each warp accumulates into its own window, summed in a fixed order.
+    __device__ void mixed_tile_mma(int tile, int tx, int ty, int tz, double* xs, double* out) const {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int g = lane >> 2, t4 = lane & 3;
+        double* acc = xs + D3a + (size_t)warp * D3a;
+        double* u1 = xs + D3a + (size_t)NW * D3a + (size_t)warp * 4 * Pa;  // [line (z, y)][x]
+        double* u2 = u1 + Pa;
+        double* e3 = u2 + Pa;  // [z][i = y][x]
+        double* e0 = e3 + Pa;
+        double* fac = xs + D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa;  // [axis][4 pos][M, K~][PP]
+        const int n = td.n;
+        for (int k = threadIdx.x; k < 3 * 4 * 2 * PP; k += blockDim.x) {
+            const int e = k % PP, w = (k / PP) % 2, pos = (k / (2 * PP)) % 4, ax = k / (8 * PP);
+            const int t = ax == 0 ? tx : (ax == 1 ? ty : tz);
+            const int el = min(t * T + pos, n - 1);
+            double v = w == 0 ? __ldg(td.M1 + (size_t)el * PP + e) : __ldg(td.Kt1 + ((size_t)ax * n + el) * PP + e);
+            if (ax == 0 && w == 1) v += td.a_mass * __ldg(td.M1 + (size_t)el * PP + e);  // a M + K~ on x
+            fac[k] = v;
+        }
+        for (int k = lane; k < D3; k += 32) acc[k] = 0.0;
+        __syncthreads();
+        const int hi = g >> 2, gi = g & 3;  // B column g: factor hi, row gi
+        const int eb = __ldg(td.tile_eptr + tile), ee = __ldg(td.tile_eptr + tile + 1);
+        for (int it = eb + warp; it < ee; it += NW) {
+            const int le = __ldg(td.tile_elem + it);
+            const int lx = le % T, ly = (le / T) % T, lz = le / (T * T);
+            const double* fx = fac + (0 * 4 + lx) * 2 * PP;  // M, then a M + K~
+            const double* fy = fac + (1 * 4 + ly) * 2 * PP;
+            const double* fz = fac + (2 * 4 + lz) * 2 * PP;
+            // B(k = t4, n = g) fragments
+            const double bx = fx[hi * PP + gi * P1 + t4];
+            const double by1 = fy[hi * PP + gi * P1 + t4];
+            const double by2 = hi ? fy[gi * P1 + t4] : 0.0;
+            const double bz1 = hi ? 0.0 : fz[gi * P1 + t4];
+            const double bz2 = hi ? 0.0 : fz[PP + gi * P1 + t4];
+            const int c0 = 2 * t4;
+            __syncwarp();  // the previous element's buffers are free
+#pragma unroll
+            for (int mb = 0; mb < 2; ++mb) {  // x pass, line = (z, y) = 8 mb + g
+                const int line = 8 * mb + g, z = line >> 2, y = line & 3;
+                const double a = xs[((lz + z) * D + (ly + y)) * D + (lx + t4)];
+                double d0 = 0.0, d1 = 0.0;
+                dmma(d0, d1, a, bx);
+                double* dst = (c0 < P1 ? u1 : u2) + line * P1 + (c0 & 3);
+                dst[0] = d0;
+                dst[1] = d1;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int mb = 0; mb < 2; ++mb) {  // y pass, line = (z, x)
+                const int line = 8 * mb + g, z = line >> 2, x = line & 3;
+                const double a1 = u1[(z * P1 + t4) * P1 + x];
+                const double a2 = u2[(z * P1 + t4) * P1 + x];
+                double d0 = 0.0, d1 = 0.0;
+                dmma(d0, d1, a1, by1);
+                dmma(d0, d1, a2, by2);
+                double* dst = (c0 < P1 ? e3 : e0) + (z * P1 + (c0 & 3)) * P1 + x;
+                dst[0] = d0;
+                dst[P1] = d1;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int mb = 0; mb < 2; ++mb) {  // z pass, line = (y, x)
+                const int line = 8 * mb + g;
+                const double a1 = e0[t4 * PP + line];
+                const double a2 = e3[t4 * PP + line];
+                double d0 = 0.0, d1 = 0.0;
+                dmma(d0, d1, a1, bz1);
+                dmma(d0, d1, a2, bz2);
+                if (c0 < P1) {  // columns 0..3 carry the element's output rows i = c0, c0 + 1
+                    const int y = line >> 2, x = line & 3;
+                    double* dst = acc + ((lz + c0) * D + (ly + y)) * D + (lx + x);
+                    dst[0] += d0;
+                    dst[D * D] += d1;
+                }
+            }
+        }
+        __syncthreads();
+        double* acc0 = xs + D3a;
+        for (int k = threadIdx.x; k < D3; k += blockDim.x) {
+            double s = 0.0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) s += acc0[(size_t)w * D3a + k];
+            out[k] = s;
+        }
+    }
+
     // Uncut elements of a mixed tile, one per half-warp (16 lanes), so a block
     // has 2 NW elements in flight; each half-warp accumulates into its own
-    // window, summed in a fixed order at the end.
+    // window, summed in a fixed order at the end.  p = 3 runs mixed_tile_mma.
     static constexpr int NH = 2 * NW;  // half-warps per block
     __device__ void mixed_tile(int tile, int tx, int ty, int tz, double* xs, double* out) const {
+        if constexpr (P1 == 4) {
+            mixed_tile_mma(tile, tx, ty, tz, xs, out);
+            return;
+        }
         const int half = threadIdx.x >> 4, hl = threadIdx.x & 15;
         const unsigned hmask = 0xffffu << (16 * ((threadIdx.x >> 4) & 1));
         double* acc = xs + D3a + (size_t)half * D3a;
@@ -952,35 +1054,42 @@ struct TileOp {
             *td.work = 0u;
             *td.work2 = 0u;
         }
-        const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-        const int gstride = gridDim.x * blockDim.x;
-        const int nneed = td.n_need;
-        const int nred = td.ext.n_red;
-        // records [0, n4) by groups of 4 lanes (all of them when there are few
-        // per thread, else only the long lists), the rest one per thread
+        // Records [0, n4) by groups of 4 lanes (every listed record when there
+        // are few per thread, else only the long lists), then the other listed
+        // records one per thread; both dealt round-robin over the blocks
+        // (record base + s owned by slot s = local * gridDim.x + block), so
+        // every block gets an equal share of the long lists at the front.  The
+        // unlisted records follow one per thread in index order (contiguous
+        // lanes read contiguous partials).
         const int q = threadIdx.x & 3;
-        const int g0 = gtid >> 2;
-        const int ng = gstride >> 2;
+        const int gstride = gridDim.x * blockDim.x, ng = gstride >> 2;
+        const int slot4 = (threadIdx.x >> 2) * gridDim.x + blockIdx.x;
+        const int slot1 = threadIdx.x * gridDim.x + blockIdx.x;
+        const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
         const int4 none = make_int4(0, 0, 0, 0);
         {
-            const int n4 = td.lane1 ? td.n_need_heavy : nneed;
-            for (int kb = g0 - (g0 & 7); kb < n4; kb += ng) {  // warp-uniform trip count
-                const int k = kb + (g0 & 7);
+            const int n4 = td.lane1 ? td.n_need_heavy : td.n_need_list;
+            for (int base = 0; base < n4; base += ng) {  // warp-uniform trip count
+                const int k = base + slot4;
                 const bool ok = k < n4;
                 const int4 rec = ok ? __ldg(td.need_rec + k) : none;
                 const double v = yfull_rec<4>(rec, q);
                 if (ok && q == 0) td.yfv[rec.x] = v;
             }
-            for (int k = n4 + gtid; k < nneed; k += gstride) {
+            for (int k = n4 + slot1; k < td.n_need_list; k += gstride) {
+                const int4 rec = __ldg(td.need_rec + k);
+                td.yfv[rec.x] = yfull_rec<1>(rec, 0);
+            }
+            for (int k = td.n_need_list + gtid; k < td.n_need; k += gstride) {
                 const int4 rec = __ldg(td.need_rec + k);
                 td.yfv[rec.x] = yfull_rec<1>(rec, 0);
             }
         }
         if (!grid_sync(gs)) return 0.0;
         double part = 0.0;
-        const int n4 = td.lane1 ? td.n_row_heavy : nred;
-        for (int jb = g0 - (g0 & 7); jb < n4; jb += ng) {
-            const int k = jb + (g0 & 7);
+        const int n4 = td.lane1 ? td.n_row_heavy : td.n_row_list;
+        for (int base = 0; base < n4; base += ng) {
+            const int k = base + slot4;
             const bool ok = k < n4;
             const int4 rec = ok ? __ldg(td.row_rec + k) : none;
             const double yj = scatter_rec<4>(rec, q);
@@ -989,9 +1098,15 @@ struct TileOp {
                 part += __ldcg(p + rec.x) * yj;
             }
         }
-        for (int k = n4 + gtid; k < nred; k += gstride) {
+        for (int k = n4 + slot1; k < td.n_row_list; k += gstride) {
             const int4 rec = __ldg(td.row_rec + k);
             const double yj = scatter_rec<1>(rec, 0);
+            y[rec.x] = yj;
+            part += __ldcg(p + rec.x) * yj;
+        }
+        for (int k = td.n_row_list + gtid; k < td.ext.n_red; k += gstride) {  // identity rows: y_j = yf of its DOF
+            const int4 rec = __ldg(td.row_rec + k);
+            const double yj = __ldcg(td.yfv + rec.y);
             y[rec.x] = yj;
             part += __ldcg(p + rec.x) * yj;
         }
