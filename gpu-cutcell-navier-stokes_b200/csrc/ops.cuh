@@ -335,39 +335,45 @@ struct TileOp {
     //   z: out = V2 Mz^T + V1 Kz^T               (line = (y, x), k = z)
     static constexpr int KS = (D + 3) / 4;
     static constexpr int NLB = (D * D + 7) / 8;
-    __device__ void full_tile_passes_mma(int tx, int ty, int tz, int tile, double* ws) const {
-        static_assert(D <= 8, "tensor-core passes need D <= 8");
+    // B fragments of the tile's six 1D factors, B(k = j, n = i) = F[i][j]:
+    // [Mx, Ax, My, Ky, Mz, Kz][k step].  Loaded before the window gather so
+    // their latency overlaps it.
+    struct TileB {
+        double f[6][KS];
+    };
+    __device__ __forceinline__ TileB tile_bfrags(int tx, int ty, int tz) const {
         const int lane = threadIdx.x & 31;
         const int g = lane >> 2, t4 = lane & 3;
         const int nta = td.nta;
+        const double* F[6] = {td.TM + (size_t)tx * D * D, td.TA + (size_t)tx * D * D,
+                              td.TM + (size_t)ty * D * D, td.TK + ((size_t)1 * nta + ty) * D * D,
+                              td.TM + (size_t)tz * D * D, td.TK + ((size_t)2 * nta + tz) * D * D};
+        TileB b;
+#pragma unroll
+        for (int m = 0; m < 6; ++m)
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks) {
+                const int i = g, j = 4 * ks + t4;
+                b.f[m][ks] = (i < D && j < D) ? __ldg(F[m] + i * D + j) : 0.0;
+            }
+        return b;
+    }
+
+    __device__ void full_tile_passes_mma(const TileB& b, int tile, double* ws) const {
+        static_assert(D <= 8, "tensor-core passes need D <= 8");
+        const int lane = threadIdx.x & 31;
+        const int g = lane >> 2, t4 = lane & 3;
         double* xs = ws;
         double* u1 = ws + D3a;
         double* u2 = u1 + D3a;
         double* v2 = u2 + D3a;
         double* v1 = xs;  // the window is dead after the x pass
-        // B fragments: B(k = j, n = i) = F[i][j]
-        auto bfrag = [&](const double* F, int ks) {
-            const int i = g, j = 4 * ks + t4;
-            return (i < D && j < D) ? __ldg(F + i * D + j) : 0.0;
-        };
-        double bMx[KS], bAx[KS], bMy[KS], bKy[KS], bMz[KS], bKz[KS];
-        {
-            const double* Mx = td.TM + (size_t)tx * D * D;
-            const double* Ax = td.TA + (size_t)tx * D * D;
-            const double* My = td.TM + (size_t)ty * D * D;
-            const double* Ky = td.TK + ((size_t)1 * nta + ty) * D * D;
-            const double* Mz = td.TM + (size_t)tz * D * D;
-            const double* Kz = td.TK + ((size_t)2 * nta + tz) * D * D;
-#pragma unroll
-            for (int ks = 0; ks < KS; ++ks) {
-                bMx[ks] = bfrag(Mx, ks);
-                bAx[ks] = bfrag(Ax, ks);
-                bMy[ks] = bfrag(My, ks);
-                bKy[ks] = bfrag(Ky, ks);
-                bMz[ks] = bfrag(Mz, ks);
-                bKz[ks] = bfrag(Kz, ks);
-            }
-        }
+        const double* bMx = b.f[0];
+        const double* bAx = b.f[1];
+        const double* bMy = b.f[2];
+        const double* bKy = b.f[3];
+        const double* bMz = b.f[4];
+        const double* bKz = b.f[5];
         constexpr int L = D * D;
         const int c0 = 2 * t4;  // this lane's two output columns c0, c0 + 1
         // x pass: A(line, j) = xs[line * D + j]
@@ -461,6 +467,8 @@ struct TileOp {
         double* u2 = u1 + D3a;
         double* v2 = u2 + D3a;
         double* v1 = xs;  // the window is dead after the x pass
+        TileB bf;
+        if constexpr (D <= 8) bf = tile_bfrags(tx, ty, tz);
         {
             int gi[KPL];
 #pragma unroll
@@ -490,7 +498,7 @@ struct TileOp {
         }
         __syncwarp();
         if constexpr (D <= 8) {
-            full_tile_passes_mma(tx, ty, tz, tile, ws);
+            full_tile_passes_mma(bf, tile, ws);
             return;
         }
         const double* Mx = td.TM + (size_t)tx * D * D;
@@ -571,14 +579,12 @@ struct TileOp {
     //   y: [e3 | e0] = U1 [My^T | Ky^T] + U2 [0 | My^T] (line = (z, x))
     //   z: s = E0 Mz^T + E3 Kz^T                        (line = (y, x))
     // Each warp accumulates into its own window, summed in a fixed order.
-    __device__ void mixed_tile_mma(int tile, int tx, int ty, int tz, double* xs, double* out) const {
+    // The tile's 1D element factors into shared memory and the per-warp
+    // windows zeroed; independent of the window gather, so phase 1 issues it
+    // before the barrier that completes the gather.
+    __device__ void mixed_prep_mma(int tx, int ty, int tz, double* xs) const {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        const int g = lane >> 2, t4 = lane & 3;
         double* acc = xs + D3a + (size_t)warp * D3a;
-        double* u1 = xs + D3a + (size_t)NW * D3a + (size_t)warp * 4 * Pa;  // [line (z, y)][x]
-        double* u2 = u1 + Pa;
-        double* e3 = u2 + Pa;  // [z][i = y][x]
-        double* e0 = e3 + Pa;
         double* fac = xs + D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa;  // [axis][4 pos][M, K~][PP]
         const int n = td.n;
         for (int k = threadIdx.x; k < 3 * 4 * 2 * PP; k += blockDim.x) {
@@ -590,7 +596,18 @@ struct TileOp {
             fac[k] = v;
         }
         for (int k = lane; k < D3; k += 32) acc[k] = 0.0;
-        __syncthreads();
+    }
+
+    // (after mixed_prep_mma and a block barrier)
+    __device__ void mixed_tile_mma(int tile, double* xs, double* out) const {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int g = lane >> 2, t4 = lane & 3;
+        double* acc = xs + D3a + (size_t)warp * D3a;
+        double* u1 = xs + D3a + (size_t)NW * D3a + (size_t)warp * 4 * Pa;  // [line (z, y)][x]
+        double* u2 = u1 + Pa;
+        double* e3 = u2 + Pa;  // [z][i = y][x]
+        double* e0 = e3 + Pa;
+        const double* fac = xs + D3a + (size_t)NW * D3a + (size_t)NW * 4 * Pa;
         const int hi = g >> 2, gi = g & 3;  // B column g: factor hi, row gi
         const int eb = __ldg(td.tile_eptr + tile), ee = __ldg(td.tile_eptr + tile + 1);
         for (int it = eb + warp; it < ee; it += NW) {
@@ -663,7 +680,7 @@ struct TileOp {
     static constexpr int NH = 2 * NW;  // half-warps per block
     __device__ void mixed_tile(int tile, int tx, int ty, int tz, double* xs, double* out) const {
         if constexpr (P1 == 4) {
-            mixed_tile_mma(tile, tx, ty, tz, xs, out);
+            mixed_tile_mma(tile, xs, out);
             return;
         }
         const int half = threadIdx.x >> 4, hl = threadIdx.x & 15;
@@ -763,14 +780,16 @@ struct TileOp {
         const int lane = threadIdx.x & 31;
         const int nb = td.nb;
         const int base = __ldg(td.cut_base + c);
+        auto gather = [&]() {
 #pragma unroll
-        for (int t = 0; t < RPL; ++t) {
-            const int k = lane + 32 * t;
-            if (k < P) {
-                const int a = k % P1, b = (k / P1) % P1, cc = k / PP;
-                xe[k] = td.ext.gather_fast(pred, base + (cc * nb + b) * nb + a);
+            for (int t = 0; t < RPL; ++t) {
+                const int k = lane + 32 * t;
+                if (k < P) {
+                    const int a = k % P1, b = (k / P1) % P1, cc = k / PP;
+                    xe[k] = td.ext.gather_fast(pred, base + (cc * nb + b) * nb + a);
+                }
             }
-        }
+        };
         const CT* A = cut_mats + (size_t)c * CUT_ENTRIES;
         acc_t acc[RPL];
 #pragma unroll
@@ -796,16 +815,16 @@ struct TileOp {
                 asm volatile("cp.async.commit_group;\n" ::: "memory");
             };
             const int tl = lane * (lane + 1) / 2;
-            issue(0);
+            issue(0);  // the first two chunks stream in while x_e is gathered
+            issue(1);
+            gather();
             __syncwarp();  // xe complete
 #pragma unroll 1
             for (int ch = 0; ch < 4; ++ch) {
-                if (ch + 1 < 4) {
-                    issue(ch + 1);
+                if (ch < 3)
                     asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-                } else {
+                else
                     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-                }
                 __syncwarp();  // every lane's pieces of chunk ch have landed
                 const CT* S = reinterpret_cast<const CT*>(bufs + (ch & 1) * SLOT);
                 if (ch == 0 || ch == 3) {  // diagonal block: the whole row of lane l
@@ -835,9 +854,11 @@ struct TileOp {
                             acc[1] += Conv<CT>::sld(S + cl * 32 + ((r + lane) & 31)) * (acc_t)xe[r];
                     }
                 }
-                __syncwarp();  // buffer (ch & 1) is refilled by issue(ch + 2)
+                __syncwarp();  // buffer (ch & 1) is free again
+                if (ch + 2 < 4) issue(ch + 2);
             }
         } else if constexpr (COLB % 16 == 0) {
+            gather();
             constexpr int BUFB = ((WS - Pa) * 8 / 2) / COLB * COLB;  // bytes per chunk buffer
             constexpr int CPC = BUFB / COLB;                         // columns per chunk
             constexpr int NCH = (P + CPC - 1) / CPC;
@@ -879,6 +900,7 @@ struct TileOp {
                 __syncwarp();  // chunk buffer (ch & 1) is refilled by issue(ch + 2)
             }
         } else {
+            gather();
             __syncwarp();
 #pragma unroll 8
             for (int col = 0; col < P; ++col) {
@@ -930,6 +952,9 @@ struct TileOp {
             const int tx = tile % nta, ty = (tile / nta) % nta, tz = tile / (nta * nta);
             double* xs = sm;
             gather_window(pred, tx, ty, tz, xs);
+            if constexpr (P1 == 4) {
+                if (item < td.n_mixed) mixed_prep_mma(tx, ty, tz, xs);
+            }
             __syncthreads();
             if (item >= td.n_mixed)
                 full_tile(tx, ty, tz, xs, td.ypart + (size_t)tile * D3);
