@@ -150,6 +150,7 @@ struct cutcell_ctx {
     double* yfv = nullptr;
     double* psmall = nullptr;
     int4* need_rec = nullptr;
+    int* cut_pos = nullptr;
     int4* row_rec = nullptr;
     // scratch
     double* dinv = nullptr;
@@ -415,8 +416,15 @@ static int build_phase2(cutcell_ctx* c, const CutcellTileDesc* t) {
         if (cptr[s + 1] < cptr[s]) return CUTCELL_E_SHAPE;
     std::vector<int> ent((size_t)nent);
     if (nent) CK(cudaMemcpy(ent.data(), t->cut_dof_ent, sizeof(int) * nent, cudaMemcpyDeviceToHost));
-    for (int e : ent)
-        if (e < 0 || e >= ncp) return CUTCELL_E_SHAPE;
+    // the lists hold every (cut element, local row) exactly once: ycut is
+    // stored in list order and each cut element writes row r to pos[c P + r]
+    if ((long)nent != ncp) return CUTCELL_E_SHAPE;
+    std::vector<int> pos((size_t)std::max<long>(ncp, 1), -1);
+    for (int k = 0; k < nent; ++k) {
+        const int e = ent[k];
+        if (e < 0 || e >= ncp || pos[e] >= 0) return CUTCELL_E_SHAPE;
+        pos[e] = k;
+    }
     std::vector<int4> nr(nneed), rr(nred);
     std::vector<char> needed((size_t)nfull, 0);
     for (int k = 0; k < nneed; ++k) {
@@ -448,6 +456,9 @@ static int build_phase2(cutcell_ctx* c, const CutcellTileDesc* t) {
     };
     order(nr, &c->td.n_need_heavy, &c->td.n_need_list);
     order(rr, &c->td.n_row_heavy, &c->td.n_row_list);
+    CK(cudaMalloc(&c->cut_pos, sizeof(int) * pos.size()));
+    CK(cudaMemcpy(c->cut_pos, pos.data(), sizeof(int) * pos.size(), cudaMemcpyHostToDevice));
+    c->td.cut_pos = c->cut_pos;
     CK(cudaMalloc(&c->need_rec, sizeof(int4) * std::max(nneed, 1)));
     CK(cudaMalloc(&c->row_rec, sizeof(int4) * std::max(nred, 1)));
     if (nneed) CK(cudaMemcpy(c->need_rec, nr.data(), sizeof(int4) * nneed, cudaMemcpyHostToDevice));
@@ -474,9 +485,11 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
         delete c;
         return st;
     }
-    const size_t nt3 = (size_t)t->n_tiles_axis * t->n_tiles_axis * t->n_tiles_axis;
-    CK(cudaMalloc(&c->ypart, nt3 * D * D * D * sizeof(double)));
-    CK(cudaMemset(c->ypart, 0, nt3 * D * D * D * sizeof(double)));
+    // DOF-major tile partials: ceil(D / tile)^3 slots per DOF, absent tiles' slots stay zero
+    const int NC = (D + t->tile - 1) / t->tile;
+    const size_t nyp = (size_t)t->n_full * NC * NC * NC;
+    CK(cudaMalloc(&c->ypart, nyp * sizeof(double)));
+    CK(cudaMemset(c->ypart, 0, nyp * sizeof(double)));
     CK(cudaMalloc(&c->ycut, ((size_t)t->n_cut * P + 1) * sizeof(double)));
     CK(cudaMemset(c->ycut, 0, ((size_t)t->n_cut * P + 1) * sizeof(double)));
     CK(cudaMalloc(&c->yfv, (size_t)t->n_full * sizeof(double)));
@@ -672,7 +685,7 @@ int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
-    void* bufs[] = {c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
                     c->p,     c->p2,    c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);

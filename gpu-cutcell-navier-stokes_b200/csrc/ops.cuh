@@ -175,8 +175,9 @@ struct TileData {
     const int* cut_dof_ptr;    // [n_slots + 1]
     const int* cut_dof_ent;    // cut * P + local
     ExtDev ext;
-    double* ypart;             // [nta^3][D^3]
-    double* ycut;              // [n_cut][P]
+    double* ypart;             // [n_full][NS] tile partials, DOF-major (slot per covering tile)
+    double* ycut;              // [n_cut * P] cut partials in DOF-list order (cut_dof_ent order)
+    const int* cut_pos;        // [n_cut * P] position of (cut, local row) in ycut
     double* yfv;               // [n_full] full-space values of the needed DOFs
     const int* need;           // [n_need] full DOFs read by the E^T scatter
     int n_need;
@@ -229,7 +230,25 @@ struct TileOp {
     // degree 3 stores its cut blocks in the symmetric split layout above
     static constexpr bool kSym = (P1 == 4);
     static constexpr int CUT_ENTRIES = kSym ? SYM64_ENTRIES : P * P;
+    // tiles covering one DOF per axis (2 for D <= 2T, 3 for p = 5) and the
+    // DOF-major partial slots per DOF
+    static constexpr int NC = (D + T - 1) / T;
+    static constexpr int NS = NC * NC * NC;
     TileData td;
+
+    // Entry k of the window of tile (tx, ty, tz) is stored at slot
+    // m = (bz NC + by) NC + bx of its DOF, b = t1 - t per axis with t1 the
+    // DOF's last covering tile (min(g / T, nta - 1)); every (DOF, tile) pair
+    // has its own slot, slots of absent tiles stay zero, and the gather sums
+    // a DOF's NS slots in order.  Entries outside the grid are dropped.
+    __device__ __forceinline__ void put_partial(int tx, int ty, int tz, int k, double v) const {
+        const int dx = k % D, dy = (k / D) % D, dz = k / (D * D);
+        const int gx = tx * T + dx, gy = ty * T + dy, gz = tz * T + dz;
+        const int nb = td.nb, nta = td.nta;
+        if (gx >= nb || gy >= nb || gz >= nb) return;
+        const int bx = min(gx / T, nta - 1) - tx, by = min(gy / T, nta - 1) - ty, bz = min(gz / T, nta - 1) - tz;
+        td.ypart[((size_t)(gz * nb + gy) * nb + gx) * NS + (bz * NC + by) * NC + bx] = v;
+    }
     const CT* __restrict__ cut_mats;
 
     // per-warp region of a warp-level item: a full tile's window and three
@@ -255,7 +274,7 @@ struct TileOp {
     }
 
     // A full tile by the whole block (few tiles per block: latency matters).
-    __device__ void full_tile(int tx, int ty, int tz, double* xs, double* out) const {
+    __device__ void full_tile(int tx, int ty, int tz, double* xs) const {
         double* u1 = xs + D3a;
         double* u2 = u1 + D3a;
         double* v1 = u2 + D3a;
@@ -312,7 +331,7 @@ struct TileOp {
                     s += __ldg(Mz + i * D + j) * v2[q] + __ldg(Kz + i * D + j) * v1[q];
                 }
             }
-            out[k] = s;
+            put_partial(tx, ty, tz, k, s);
         }
     }
 
@@ -429,7 +448,8 @@ struct TileOp {
         }
         __syncwarp();
         // z pass: line = (y, x), A(line, j) = V[j * D * D + line]
-        double* out = td.ypart + (size_t)tile * D3;
+        const int nta = td.nta;
+        const int tx = tile % nta, ty = (tile / nta) % nta, tz = tile / (nta * nta);
 #pragma unroll 1
         for (int mb = 0; mb < NLB; ++mb) {
             const int line = 8 * mb + g;
@@ -444,8 +464,8 @@ struct TileOp {
                 dmma(p0, p1, a1, bKz[ks]);
             }
             if (line < L) {
-                if (c0 < D) out[c0 * L + line] = p0;
-                if (c0 + 1 < D) out[(c0 + 1) * L + line] = p1;
+                if (c0 < D) put_partial(tx, ty, tz, c0 * L + line, p0);
+                if (c0 + 1 < D) put_partial(tx, ty, tz, (c0 + 1) * L + line, p1);
             }
         }
         __syncwarp();
@@ -549,7 +569,6 @@ struct TileOp {
             }
         }
         __syncwarp();
-        double* out = td.ypart + (size_t)tile * D3;
 #pragma unroll
         for (int t = 0; t < KPL; ++t) {
             const int k = lane + 32 * t;
@@ -564,7 +583,7 @@ struct TileOp {
                         s += __ldg(Mz + i * D + j) * v2[q] + __ldg(Kz + i * D + j) * v1[q];
                     }
                 }
-                out[k] = s;
+                put_partial(tx, ty, tz, k, s);
             }
         }
         __syncwarp();
@@ -599,7 +618,7 @@ struct TileOp {
     }
 
     // (after mixed_prep_mma and a block barrier)
-    __device__ void mixed_tile_mma(int tile, double* xs, double* out) const {
+    __device__ void mixed_tile_mma(int tile, int tx, int ty, int tz, double* xs) const {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int g = lane >> 2, t4 = lane & 3;
         double* acc = xs + D3a + (size_t)warp * D3a;
@@ -670,7 +689,7 @@ struct TileOp {
             double s = 0.0;
 #pragma unroll
             for (int w = 0; w < NW; ++w) s += acc0[(size_t)w * D3a + k];
-            out[k] = s;
+            put_partial(tx, ty, tz, k, s);
         }
     }
 
@@ -678,9 +697,9 @@ struct TileOp {
     // has 2 NW elements in flight; each half-warp accumulates into its own
     // window, summed in a fixed order at the end.  p = 3 runs mixed_tile_mma.
     static constexpr int NH = 2 * NW;  // half-warps per block
-    __device__ void mixed_tile(int tile, int tx, int ty, int tz, double* xs, double* out) const {
+    __device__ void mixed_tile(int tile, int tx, int ty, int tz, double* xs) const {
         if constexpr (P1 == 4) {
-            mixed_tile_mma(tile, xs, out);
+            mixed_tile_mma(tile, tx, ty, tz, xs);
             return;
         }
         const int half = threadIdx.x >> 4, hl = threadIdx.x & 15;
@@ -760,7 +779,7 @@ struct TileOp {
             double s = 0.0;
 #pragma unroll
             for (int w = 0; w < NH; ++w) s += acc0[(size_t)w * D3a + k];
-            out[k] = s;
+            put_partial(tx, ty, tz, k, s);
         }
     }
 
@@ -913,7 +932,7 @@ struct TileOp {
         }
 #pragma unroll
         for (int q = 0; q < RPL; ++q)
-            if (lane + 32 * q < P) td.ycut[(size_t)c * P + lane + 32 * q] = (double)acc[q];
+            if (lane + 32 * q < P) td.ycut[__ldg(td.cut_pos + (size_t)c * P + lane + 32 * q)] = (double)acc[q];
         __syncwarp();
     }
 
@@ -957,9 +976,9 @@ struct TileOp {
             }
             __syncthreads();
             if (item >= td.n_mixed)
-                full_tile(tx, ty, tz, xs, td.ypart + (size_t)tile * D3);
+                full_tile(tx, ty, tz, xs);
             else
-                mixed_tile(tile, tx, ty, tz, xs, td.ypart + (size_t)tile * D3);
+                mixed_tile(tile, tx, ty, tz, xs);
             __syncthreads();
         }
         // warp-level items: cut elements, then (if warp-level) full tiles
@@ -979,39 +998,28 @@ struct TileOp {
         __syncthreads();
     }
 
-    // full-space value of DOF rec.x: its (up to 8) tile partials and its cut
-    // partials [rec.z, rec.w), summed by G = 1 thread or by the q-th of a
-    // group of G = 4 lanes (partials interleaved over the lanes, then a fixed
-    // xor tree, so every lane of the group returns the same bits).
+    // full-space value of DOF rec.x: its NS tile-partial slots and its cut
+    // partials [rec.z, rec.w) of ycut, both contiguous, summed by G = 1 thread
+    // or by the q-th of a group of G = 4 lanes (partials interleaved over the
+    // lanes, then a fixed xor tree, so every lane of the group returns the
+    // same bits).
     template <int G>
     __device__ __forceinline__ double yfull_rec(const int4 rec, int q) const {
-        const int i = rec.x;
-        const int nb = td.nb, nta = td.nta;
-        const int ix = i % nb, iy = (i / nb) % nb, iz = i / (nb * nb);
-        const int t1x = min(ix / T, nta - 1), t1y = min(iy / T, nta - 1), t1z = min(iz / T, nta - 1);
+        const double* yp = td.ypart + (size_t)rec.x * NS;
         double s = 0.0;
 #pragma unroll
-        for (int m = q; m < 8; m += G) {
-            const int tz = t1z - ((m >> 2) & 1), ty = t1y - ((m >> 1) & 1), tx = t1x - (m & 1);
-            if (tz < 0 || ty < 0 || tx < 0) continue;
-            if (iz - tz * T >= D || iy - ty * T >= D || ix - tx * T >= D) continue;
-            const int tile = (tz * nta + ty) * nta + tx;
-            s += __ldcg(td.ypart + (size_t)tile * D3 + ((iz - tz * T) * D + (iy - ty * T)) * D + (ix - tx * T));
-        }
+        for (int m = q; m < NS; m += G) s += __ldcg(yp + m);
         int k = rec.z + q;
         if constexpr (G == 1) {
-            for (; k + 4 <= rec.w; k += 4) {  // four entries' loads in flight
-                int e[4];
+            for (; k + 4 <= rec.w; k += 4) {  // four loads in flight
                 double v[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) e[u] = __ldg(td.cut_dof_ent + k + u);
-#pragma unroll
-                for (int u = 0; u < 4; ++u) v[u] = __ldcg(td.ycut + e[u]);
+                for (int u = 0; u < 4; ++u) v[u] = __ldcg(td.ycut + k + u);
 #pragma unroll
                 for (int u = 0; u < 4; ++u) s += v[u];
             }
         }
-        for (; k < rec.w; k += G) s += __ldcg(td.ycut + __ldg(td.cut_dof_ent + k));
+        for (; k < rec.w; k += G) s += __ldcg(td.ycut + k);
         if constexpr (G == 4) {
             s += __shfl_xor_sync(0xffffffffu, s, 1);
             s += __shfl_xor_sync(0xffffffffu, s, 2);

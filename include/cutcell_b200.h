@@ -89,7 +89,8 @@ typedef struct {
     const int32_t* cut_base;   /* [n_cut] full index of each cut element's first DOF */
     const int32_t* cut_dof_slot; /* [n_full] slot in the DOF -> cut-element list, -1 if none */
     const int32_t* cut_dof_ptr;  /* [n_slots + 1] */
-    const int32_t* cut_dof_ent;  /* cut * (p+1)^3 + local row, ascending per slot */
+    const int32_t* cut_dof_ent;  /* cut * (p+1)^3 + local row, ascending per slot; every
+                                    (cut, local row) appears exactly once */
     const int32_t* need;         /* [n_need] full DOF indices */
     const int32_t* red_of_full;
     const int32_t* small_slot;

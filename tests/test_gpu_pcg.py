@@ -107,6 +107,21 @@ def test_matrix_free_apply_matches_oracle(torch_cuda, kind, n, p):
     op_.close()
 
 
+def test_matrix_free_apply_three_tiles_per_axis(torch_cuda):
+    """p = 5: the 9-wide tile windows overlap so that interior DOFs lie in
+    three tiles per axis (27 partial slots); n = 10 has three tiles per axis."""
+    from cutcell_b200.operator import CutCellOperator
+
+    prob, ext, A_full, A_red, b = system("plane", 10, 5)
+    op_ = CutCellOperator(prob, ext)
+    assert op_.layout.n_tiles_axis == 3
+    x = np.random.default_rng(9).standard_normal(ext.n_red)
+    ref = A_red @ x
+    y = op_.apply(x, "fp64").cpu().numpy()
+    assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 1e-12
+    op_.close()
+
+
 @pytest.mark.parametrize("kind,n,p", CASES[:3])
 def test_matrix_free_pcg_matches_oracle(torch_cuda, kind, n, p):
     from cutcell_b200 import solve_spd
