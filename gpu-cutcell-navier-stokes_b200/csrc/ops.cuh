@@ -175,7 +175,7 @@ struct TileData {
     const int* cut_dof_ptr;    // [n_slots + 1]
     const int* cut_dof_ent;    // cut * P + local
     ExtDev ext;
-    double* ypart;             // [n_full][NS] tile partials, DOF-major (slot per covering tile)
+    double* ypart;             // [NS][n_full] tile partials: one plane per covering-tile slot
     double* ycut;              // [n_cut * P] cut partials in DOF-list order (cut_dof_ent order)
     const int* cut_pos;        // [n_cut * P] position of (cut, local row) in ycut
     double* yfv;               // [n_full] full-space values of the needed DOFs
@@ -236,18 +236,20 @@ struct TileOp {
     static constexpr int NS = NC * NC * NC;
     TileData td;
 
-    // Entry k of the window of tile (tx, ty, tz) is stored at slot
-    // m = (bz NC + by) NC + bx of its DOF, b = t1 - t per axis with t1 the
+    // Entry k of the window of tile (tx, ty, tz) is stored in slot plane
+    // m = (bz NC + by) NC + bx at its DOF, b = t1 - t per axis with t1 the
     // DOF's last covering tile (min(g / T, nta - 1)); every (DOF, tile) pair
     // has its own slot, slots of absent tiles stay zero, and the gather sums
-    // a DOF's NS slots in order.  Entries outside the grid are dropped.
+    // a DOF's NS slots in order.  Entries outside the grid are dropped.  Runs
+    // of x-neighbours land in consecutive addresses of one plane, and so do
+    // the gather's loads for consecutive DOFs.
     __device__ __forceinline__ void put_partial(int tx, int ty, int tz, int k, double v) const {
         const int dx = k % D, dy = (k / D) % D, dz = k / (D * D);
         const int gx = tx * T + dx, gy = ty * T + dy, gz = tz * T + dz;
         const int nb = td.nb, nta = td.nta;
         if (gx >= nb || gy >= nb || gz >= nb) return;
         const int bx = min(gx / T, nta - 1) - tx, by = min(gy / T, nta - 1) - ty, bz = min(gz / T, nta - 1) - tz;
-        td.ypart[((size_t)(gz * nb + gy) * nb + gx) * NS + (bz * NC + by) * NC + bx] = v;
+        td.ypart[(size_t)((bz * NC + by) * NC + bx) * td.ext.n_full + (gz * nb + gy) * nb + gx] = v;
     }
     const CT* __restrict__ cut_mats;
 
@@ -998,17 +1000,18 @@ struct TileOp {
         __syncthreads();
     }
 
-    // full-space value of DOF rec.x: its NS tile-partial slots and its cut
-    // partials [rec.z, rec.w) of ycut, both contiguous, summed by G = 1 thread
+    // full-space value of DOF rec.x: its NS tile-partial slots (one per plane)
+    // and its cut partials [rec.z, rec.w) of ycut (contiguous), summed by G = 1 thread
     // or by the q-th of a group of G = 4 lanes (partials interleaved over the
     // lanes, then a fixed xor tree, so every lane of the group returns the
     // same bits).
     template <int G>
     __device__ __forceinline__ double yfull_rec(const int4 rec, int q) const {
-        const double* yp = td.ypart + (size_t)rec.x * NS;
+        const double* yp = td.ypart + rec.x;
+        const size_t plane = td.ext.n_full;
         double s = 0.0;
 #pragma unroll
-        for (int m = q; m < NS; m += G) s += __ldcg(yp + m);
+        for (int m = q; m < NS; m += G) s += __ldcg(yp + m * plane);
         int k = rec.z + q;
         if constexpr (G == 1) {
             for (; k + 4 <= rec.w; k += 4) {  // four loads in flight
