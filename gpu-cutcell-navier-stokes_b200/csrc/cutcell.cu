@@ -385,7 +385,8 @@ int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const 
 }
 
 // Phase-2 work records, built once on the host from the descriptor's lists:
-//   need_rec[k] = {full DOF i, 0, first, end of i's cut partials in cut_dof_ent}
+//   need_rec[k] = {full DOF i, row j whose y_j is i's value alone (no E^T
+//                  entries) or -1, first, end of i's cut partials in ycut}
 //   row_rec[k]  = {reduced row j, full DOF of j, first, end of j's E^T entries}
 // The records with a list come first, by list length in buckets of 4 entries,
 // longest first; the records without one (plain tile-partial sums and
@@ -429,9 +430,10 @@ static int build_phase2(cutcell_ctx* c, const CutcellTileDesc* t) {
     std::vector<char> needed((size_t)nfull, 0);
     for (int k = 0; k < nneed; ++k) {
         const int i = need[k];
-        if (i < 0 || i >= nfull) return CUTCELL_E_SHAPE;
+        if (i < 0 || i >= nfull || needed[i]) return CUTCELL_E_SHAPE;  // in range, listed once
+        if (rof[i] < -1 || rof[i] >= nred) return CUTCELL_E_SHAPE;
         const int s = slot[i];
-        nr[k] = s >= 0 ? make_int4(i, 0, cptr[s], cptr[s + 1]) : make_int4(i, 0, 0, 0);
+        nr[k] = s >= 0 ? make_int4(i, -1, cptr[s], cptr[s + 1]) : make_int4(i, -1, 0, 0);
         needed[i] = 1;
     }
     if (tptr[0] != 0) return CUTCELL_E_SHAPE;
@@ -444,8 +446,12 @@ static int build_phase2(cutcell_ctx* c, const CutcellTileDesc* t) {
     std::vector<int> trow((size_t)tptr[nred]);
     if (!trow.empty())
         CK(cudaMemcpy(trow.data(), t->smallT_row, sizeof(int) * trow.size(), cudaMemcpyDeviceToHost));
-    for (int i : trow)
-        if (i < 0 || i >= nfull || !needed[i]) return CUTCELL_E_SHAPE;
+    for (int i : trow)  // only small (non-identity) DOFs are read by other rows
+        if (i < 0 || i >= nfull || !needed[i] || rof[i] >= 0) return CUTCELL_E_SHAPE;
+    // a row without E^T entries is y_j = yf of its own DOF: the gather of
+    // that DOF writes y_j directly (need_rec.y = j), the scatter skips it
+    for (int4& r : nr)
+        if (rof[r.x] >= 0 && tptr[rof[r.x] + 1] == tptr[rof[r.x]]) r.y = rof[r.x];
     auto order = [](std::vector<int4>& v, int* heavy, int* listed) {
         auto key = [](const int4& a) { return a.w > a.z ? 1 + (a.w - a.z) / 4 : 0; };
         std::stable_sort(v.begin(), v.end(), [&](const int4& a, const int4& b) { return key(a) > key(b); });

@@ -183,7 +183,7 @@ struct TileData {
     int n_need;
     // phase-2 records (built by the host at create): those with a list first,
     // longest first, then those without, in index order
-    const int4* need_rec;      // [n_need] {full DOF, 0, cut partials [z, w) in cut_dof_ent}
+    const int4* need_rec;      // [n_need] {full DOF, row it completes or -1, cut partials [z, w) in ycut}
     const int4* row_rec;       // [n_red] {reduced row, its full DOF, E^T entries [z, w)}
     int n_need_heavy;          // leading records whose lists are long (4 lanes each when lane1)
     int n_row_heavy;
@@ -1102,7 +1102,18 @@ struct TileOp {
         const int slot4 = (threadIdx.x >> 2) * gridDim.x + blockIdx.x;
         const int slot1 = threadIdx.x * gridDim.x + blockIdx.x;
         const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-        const int4 none = make_int4(0, 0, 0, 0);
+        const int4 none = make_int4(0, -1, 0, 0);
+        // a DOF whose row has no E^T entries completes that row here: y_j and
+        // its p.y term; the others go to yfv for the scatter
+        double part = 0.0;
+        auto finish = [&](const int4& rec, double v) {
+            if (rec.y >= 0) {
+                y[rec.y] = v;
+                part += __ldcg(p + rec.y) * v;
+            } else {
+                td.yfv[rec.x] = v;
+            }
+        };
         {
             const int n4 = td.lane1 ? td.n_need_heavy : td.n_need_list;
             for (int base = 0; base < n4; base += ng) {  // warp-uniform trip count
@@ -1110,24 +1121,23 @@ struct TileOp {
                 const bool ok = k < n4;
                 const int4 rec = ok ? __ldg(td.need_rec + k) : none;
                 const double v = yfull_rec<4>(rec, q);
-                if (ok && q == 0) td.yfv[rec.x] = v;
+                if (ok && q == 0) finish(rec, v);
             }
             for (int k = n4 + slot1; k < td.n_need_list; k += gstride) {
                 const int4 rec = __ldg(td.need_rec + k);
-                td.yfv[rec.x] = yfull_rec<1>(rec, 0);
+                finish(rec, yfull_rec<1>(rec, 0));
             }
             for (int k = td.n_need_list + gtid; k < td.n_need; k += gstride) {
                 const int4 rec = __ldg(td.need_rec + k);
-                td.yfv[rec.x] = yfull_rec<1>(rec, 0);
+                finish(rec, yfull_rec<1>(rec, 0));
             }
         }
         if (!grid_sync(gs)) return 0.0;
-        double part = 0.0;
         const int n4 = td.lane1 ? td.n_row_heavy : td.n_row_list;
         for (int base = 0; base < n4; base += ng) {
             const int k = base + slot4;
             const bool ok = k < n4;
-            const int4 rec = ok ? __ldg(td.row_rec + k) : none;
+            const int4 rec = ok ? __ldg(td.row_rec + k) : make_int4(0, 0, 0, 0);  // idle groups read DOF 0
             const double yj = scatter_rec<4>(rec, q);
             if (ok && q == 0) {
                 y[rec.x] = yj;
@@ -1140,12 +1150,7 @@ struct TileOp {
             y[rec.x] = yj;
             part += __ldcg(p + rec.x) * yj;
         }
-        for (int k = td.n_row_list + gtid; k < td.ext.n_red; k += gstride) {  // identity rows: y_j = yf of its DOF
-            const int4 rec = __ldg(td.row_rec + k);
-            const double yj = __ldcg(td.yfv + rec.y);
-            y[rec.x] = yj;
-            part += __ldcg(p + rec.x) * yj;
-        }
+        // rows [n_row_list, n_red) have no E^T entries and were completed above
         return part;
     }
 };
