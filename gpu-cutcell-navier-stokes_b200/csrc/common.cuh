@@ -34,17 +34,26 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     return v;
 }
 
+__device__ __forceinline__ unsigned atom_add_release_u32(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Grid barrier for a cooperative (co-resident) grid: every block adds to one
 // arrival word, block 0 adds 2^31 - (nblocks - 1) so the word's top bit flips
 // exactly when the last block arrives; waiters poll the word with acquire
 // loads.  No reset is needed between barriers.  Every wait is bounded: after
 // CUTCELL_BARRIER_CYCLES the error word is set and all blocks leave their loops.
+// Ordering: the block barrier makes the block's writes precede thread 0's
+// release add (release is cumulative); the acquire load that sees the flip
+// and the closing block barrier make every other block's writes visible to
+// all threads, without full fences on either side.
 __device__ __forceinline__ bool grid_sync(const GridSync& gs) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned add = (blockIdx.x == 0) ? (0x80000000u - (gs.nblocks - 1u)) : 1u;
-        __threadfence();
-        const unsigned old = atomicAdd(gs.count, add);
+        const unsigned old = atom_add_release_u32(gs.count, add);
         long long t0 = clock64();
         unsigned spins = 0;
         while (((old ^ ld_acquire_u32(gs.count)) & 0x80000000u) == 0u) {
@@ -56,7 +65,6 @@ __device__ __forceinline__ bool grid_sync(const GridSync& gs) {
                 if (*((volatile int*)gs.err) != 0) break;
             }
         }
-        __threadfence();
     }
     __syncthreads();
     return grid_error(gs) == 0;
