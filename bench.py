@@ -118,8 +118,8 @@ class ClockSampler:
 # one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the same
 # command; None where no capture was made for that configuration.
 NCU_TRAFFIC = {
-    ("sphere", 32, 3): 35.15e6 + 1.06e6,   # pcg_kernel, one whole solve
-    ("apply", 64, 3): 149.6e6 + 7.4e6,     # apply_kernel, one apply
+    ("sphere", 32, 3): 37.10e6 + 1.50e6,   # pcg_kernel, one whole solve
+    ("apply", 64, 3): 157.17e6 + 6.61e6,   # apply_kernel, one apply
     ("batch", 72): 17.6e6,                 # batch_pcg_kernel, one launch
     ("hill-step",): 161.7e6 + 32.6e6,      # hill_segment_kernel, one 3-component advection
 }
