@@ -133,6 +133,19 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def host_cpu() -> dict:
+    """The host the CPU baseline ran on: logical CPUs and the CPU model name."""
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count() or 1, "cpu_model": model}
+
+
 def cut_block_entries(P: int) -> int:
     """Stored entries per cut-element block: degree 3 (P = 64) keeps the upper
     triangle of its symmetric block (P(P+1)/2), other degrees the dense block."""
@@ -145,7 +158,7 @@ def algorithmic_bytes_per_iter(prob, ext, prec: str) -> float:
     N = ext.n_red
     nnz_small = int(ext.E[ext.small_support].nnz)
     b_e = 2 * (4 + 8) * nnz_small + 4 * ext.n_full
-    s = {"fp64": 8, "fp32-ir": 4, "bf16-ir": 2}[prec]
+    s = {"fp64": 8, "fp32-ir": 4, "bf16-ir": 4}[prec]  # bf16-ir: two BF16 planes per entry
     b_op = prob.cut_ids.size * cut_block_entries(prob.P) * s
     return 13 * 8 * N + b_e + b_op
 
@@ -203,7 +216,7 @@ def run_batch_reference(args, rank, world):
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cuts and right-hand sides)",
         "config": {"workload": f"{len(systems)} oblique 2D cut systems, one solve_cpu_cg each"},
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
-                         "sample": f"all {len(systems)} systems per step, sequential SciPy CG"},
+                         "sample": f"all {len(systems)} systems per step, sequential SciPy CG", **host_cpu()},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -340,7 +353,7 @@ def run_batch(args, rank, world, local):
             k += 1
         cs = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": k / cs, "unit": "solves/s", "cores": 1, "kind": "port",
-                                "sample": f"first {k} of the {len(systems)} systems, sequential SciPy CG"}
+                                "sample": f"first {k} of the {len(systems)} systems, sequential SciPy CG", **host_cpu()}
     if rank == 0:
         print(json.dumps(line), flush=True)
     bs.close()
@@ -391,7 +404,7 @@ def run_reference(args, rank, world):
         "dtype": "f64",
         "data": "synthetic (seeded geometry, manufactured forcing)",
         "config": {"workload": f"sphere-cut Poisson p={args.p} n={args.n} r={args.radius}", "n_red": ext.n_red, "nnz": int(A.nnz), "iterations": it},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": "full solve per step (SciPy CSR SpMV is single-threaded)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": "full solve per step (SciPy CSR SpMV is single-threaded)", **host_cpu()},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -672,7 +685,7 @@ def main():
         if prec == "learned":
             solve_kw = {"precision": "fp64", "preconditioner": "jacobi+learned"}
         elif prec != "fp64":
-            op.set_refinement(1e-2 if prec == "bf16-ir" else 1e-4)
+            op.set_refinement(0.1)
         for _ in range(args.warmup):
             x, rep = op.solve_device(b, tol=TOL, maxiter=20000, **solve_kw)
         barrier()
@@ -783,6 +796,7 @@ def main():
         line["cpu_baseline"] = {
             "value": cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"one full SciPy Jacobi-CG solve on the assembled CSR (nnz {A.nnz}, {cpu_it} iterations)",
+            **host_cpu(),
         }
         line["config"]["cpu_rel_err_vs_gpu_fp64"] = float(np.linalg.norm(xc - ref_x) / np.linalg.norm(xc))
     if rank == 0:

@@ -13,16 +13,29 @@
 #endif
 #define CUTCELL_WARPS (CUTCELL_BLOCK / 32)
 
-// Grid barrier wait limit in SM clock cycles (about one second at 2 GHz).  A
+// Grid barrier wait limit.  Waits are measured on the device's global timer
+// (wall-clock nanoseconds, unaffected by SM clocks or by a block being
+// descheduled), and the limit is a runtime value carried in GridSync: the
+// library default is 10 s, changed by cutcell_set_wait_limit or by the
+// environment variable CUTCELL_WAIT_LIMIT_S read at the first launch.  A
 // barrier that runs out sets CUTCELL_E_BARRIER and every block leaves its loop.
-#define CUTCELL_BARRIER_CYCLES 2000000000LL
+#define CUTCELL_DEFAULT_WAIT_LIMIT_S 10.0
+
+// Host side: the current limit in nanoseconds (defined in cutcell.cu).
+unsigned long long cutcell_internal_wait_limit_ns();
 
 struct GridSync {
     unsigned* count;  // arrival word (own 128-byte line); its top bit flips once per barrier
-    unsigned* gen;    // unused (kept for layout compatibility)
+    unsigned long long limit_ns;  // bounded-wait limit (global-timer nanoseconds)
     int* err;         // error word (own 128-byte line)
     unsigned nblocks;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ int grid_error(const GridSync& gs) {
     return *((volatile int*)gs.err);
@@ -44,7 +57,7 @@ __device__ __forceinline__ unsigned atom_add_release_u32(unsigned* p, unsigned v
 // arrival word, block 0 adds 2^31 - (nblocks - 1) so the word's top bit flips
 // exactly when the last block arrives; waiters poll the word with acquire
 // loads.  No reset is needed between barriers.  Every wait is bounded: after
-// CUTCELL_BARRIER_CYCLES the error word is set and all blocks leave their loops.
+// gs.limit_ns of global time the error word is set and all blocks leave their loops.
 // Ordering: the block barrier makes the block's writes precede thread 0's
 // release add (release is cumulative); the acquire load that sees the flip
 // and the closing block barrier make every other block's writes visible to
@@ -54,11 +67,11 @@ __device__ __forceinline__ bool grid_sync(const GridSync& gs) {
     if (threadIdx.x == 0) {
         const unsigned add = (blockIdx.x == 0) ? (0x80000000u - (gs.nblocks - 1u)) : 1u;
         const unsigned old = atom_add_release_u32(gs.count, add);
-        long long t0 = clock64();
+        const unsigned long long t0 = global_ns();
         unsigned spins = 0;
         while (((old ^ ld_acquire_u32(gs.count)) & 0x80000000u) == 0u) {
             if ((++spins & 1023u) == 0u) {
-                if (clock64() - t0 > CUTCELL_BARRIER_CYCLES) {
+                if (global_ns() - t0 > gs.limit_ns) {
                     atomicExch(gs.err, CUTCELL_E_BARRIER);
                     break;
                 }
@@ -123,6 +136,29 @@ template <> struct Conv<__nv_bfloat16> {
     typedef float acc;
     __device__ __forceinline__ static float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
     __device__ __forceinline__ static float sld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+};
+
+// Two-plane BF16 storage of the BF16 operator form: a value v is kept as
+// hi = bf16(v) and lo = bf16(v - hi), 4 bytes, read back as float(hi) +
+// float(lo) (about 16 significant bits) and accumulated in FP32.  One BF16
+// plane alone (8 bits) perturbs the weak-penalty cut blocks, whose Nitsche
+// penalty entries are two orders of magnitude above their stiffness entries,
+// by more than the smallest eigenvalues of the Jacobi-scaled system, and the
+// refinement then stagnates.
+struct __align__(4) bf16x2_t {
+    __nv_bfloat16 hi, lo;
+};
+template <> struct Conv<bf16x2_t> {
+    typedef float acc;
+    __device__ __forceinline__ static float unpack(unsigned u) {
+        return __uint_as_float(u << 16) + __uint_as_float(u & 0xffff0000u);
+    }
+    __device__ __forceinline__ static float ld(const bf16x2_t* p) {
+        return unpack(__ldg(reinterpret_cast<const unsigned*>(p)));
+    }
+    __device__ __forceinline__ static float sld(const bf16x2_t* p) {
+        return unpack(*reinterpret_cast<const unsigned*>(p));
+    }
 };
 
 // Optional self-checks (build with -DCUTCELL_DEBUG_CHECKS): a failed check

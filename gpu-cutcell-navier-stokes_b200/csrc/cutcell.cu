@@ -1,8 +1,10 @@
 // C ABI of libcutcell_b200.so: contexts, cooperative launches, status codes.
 // The persistent kernels live in pcg.cuh / ops.cuh.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 #include <cstring>
 #include <string>
@@ -10,6 +12,7 @@
 #include "pcg.cuh"
 #include "learned.cuh"
 #include "fastdiag.cuh"
+#include "kron.cuh"
 
 namespace {
 
@@ -26,7 +29,7 @@ int cuda_fail(cudaError_t e, const char* what) {
         if (_e != cudaSuccess) return cuda_fail(_e, #call); \
     } while (0)
 
-enum { KIND_CSR = 0, KIND_TILES = 1 };
+enum { KIND_CSR = 0, KIND_TILES = 1, KIND_KRON = 2 };
 constexpr int BAR_WORDS = 160;
 
 __global__ void csr_diag_inv_kernel(int n, const int* ptr, const int* idx, const double* val, double* dinv) {
@@ -37,6 +40,10 @@ __global__ void csr_diag_inv_kernel(int n, const int* ptr, const int* idx, const
         dinv[row] = (fabs(d) > 0.0) ? 1.0 / d : 1.0;
     }
 }
+
+// One grid barrier over a cooperative grid that waits for `arrivals`
+// arrivals (the diagnostic of cutcell_barrier_selftest).
+__global__ void barrier_probe_kernel(GridSync gs) { grid_sync(gs); }
 
 __global__ void fill_kernel(int n, double v, double* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = v;
@@ -54,9 +61,14 @@ __global__ void to_f32_kernel(size_t n, const double* in, float* out) {
         out[i] = (float)in[i];
 }
 
-__global__ void to_bf16_kernel(size_t n, const double* in, __nv_bfloat16* out) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        out[i] = __float2bfloat16((float)in[i]);
+// two-plane BF16: hi = bf16(v), lo = bf16(v - hi)
+__global__ void to_bf16x2_kernel(size_t n, const double* in, bf16x2_t* out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = in[i];
+        const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
+        out[i].hi = h;
+        out[i].lo = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
+    }
 }
 
 // Dense symmetric 64 x 64 cut blocks -> the 2080-entry split storage of
@@ -136,15 +148,15 @@ struct cutcell_ctx {
     // CSR
     CsrOp<double> csr64;
     CsrOp<float> csr32;
-    CsrOp<__nv_bfloat16> csr16;
+    CsrOp<bf16x2_t> csr16;
     float* val32 = nullptr;
-    __nv_bfloat16* val16 = nullptr;
+    bf16x2_t* val16 = nullptr;
     // tiles
     TileData td;
     const double* cut64 = nullptr;
     double* cutsym = nullptr;  // degree 3: owned split-storage copy of the cut blocks
     float* cut32 = nullptr;
-    __nv_bfloat16* cut16 = nullptr;
+    bf16x2_t* cut16 = nullptr;
     double* ypart = nullptr;
     double* ycut = nullptr;
     double* yfv = nullptr;
@@ -152,6 +164,12 @@ struct cutcell_ctx {
     int4* need_rec = nullptr;
     int* cut_pos = nullptr;
     int4* row_rec = nullptr;
+    // Kronecker cut box: banded reduced 1D factors [axis][H, K, Q, S, A]
+    int kn[3] = {0, 0, 0};
+    KronBand kb[3][5];
+    int* klo = nullptr;
+    double* kband = nullptr;
+    double* kscratch = nullptr;  // U1 U2 V1 V2
     // scratch
     double* dinv = nullptr;
     double* ones = nullptr;
@@ -171,10 +189,10 @@ struct cutcell_ctx {
     PatchMap pmap = {0, nullptr, nullptr, nullptr};
     double* zl = nullptr;
     double* rold = nullptr;
-    // refinement
-    double inner_tol = 1e-4;
-    int inner_maxiter = 100000;
-    int max_outer = 50;
+    // reduced-precision forms: residual-replacement factor and cap
+    double inner_tol = 0.1;
+    int inner_maxiter = 0;
+    int max_outer = 200;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -212,7 +230,7 @@ static int ensure_part(cutcell_ctx* c, K kernel, size_t smem, int* blocks) {
 static GridSync make_gs(cutcell_ctx* c, int blocks) {
     GridSync gs;
     gs.count = c->bar;
-    gs.gen = c->bar;
+    gs.limit_ns = cutcell_internal_wait_limit_ns();
     gs.err = (int*)(c->bar + 32);
     gs.nblocks = (unsigned)blocks;
     return gs;
@@ -248,9 +266,9 @@ static int run_plain(cutcell_ctx* c, const Op& op, size_t smem, SolveArgs& a, cu
 }
 
 template <class OpHi, class OpLo>
-static int run_ir(cutcell_ctx* c, const OpHi& hi, const OpLo& lo, size_t smem, SolveArgs& a, cudaStream_t s,
+static int run_ru(cutcell_ctx* c, const OpHi& hi, const OpLo& lo, size_t smem, SolveArgs& a, cudaStream_t s,
                   int* blocks) {
-    auto kern = ir_kernel<OpHi, OpLo>;
+    auto kern = ru_kernel<OpHi, OpLo>;
     int st = ensure_part(c, kern, smem, blocks);
     if (st) return st;
     a.gs = make_gs(c, *blocks);
@@ -288,16 +306,17 @@ static int run_apply(cutcell_ctx* c, const Op& op, size_t smem, const double* x,
 }
 
 // mode 0: solve (plain or refinement), mode 1: one apply
-// Reduced-precision refinement is built for p >= 3 only: the fused
+// Reduced-precision refinement is built for p >= 3 only: an earlier fused
 // refinement kernel instantiated for p = 2 faulted (misaligned address) on
-// the B200 while the same code with self-checks compiled in ran clean; until
-// the cause is found that instantiation is not built.
+// the B200 while the same code with self-checks compiled in ran clean, and
+// reading the p = 2 paths did not show the cause; until it is found the
+// p = 2 reduced-precision instantiations are not built.
 template <int P1>
 static int tiles_run(cutcell_ctx* c, int mode, int precision, SolveArgs* a, const double* x, double* y, cudaStream_t s,
                      int* blocks) {
     TileOp<double, P1> o64{c->td, c->cut64};
     TileOp<float, P1> o32{c->td, c->cut32};
-    TileOp<__nv_bfloat16, P1> o16{c->td, c->cut16};
+    TileOp<bf16x2_t, P1> o16{c->td, c->cut16};
     const size_t sm = TileOp<double, P1>::smem_bytes();
     if (mode == 2) return run_fcg(c, o64, sm, *a, s, blocks);
     if (mode == 1) {
@@ -307,8 +326,8 @@ static int tiles_run(cutcell_ctx* c, int mode, int precision, SolveArgs* a, cons
     }
     if (precision == CUTCELL_FP64) return run_plain(c, o64, sm, *a, s, blocks);
     if constexpr (P1 >= 4) {
-        if (precision == CUTCELL_FP32_IR) return run_ir(c, o64, o32, sm, *a, s, blocks);
-        return run_ir(c, o64, o16, sm, *a, s, blocks);
+        if (precision == CUTCELL_FP32_IR) return run_ru(c, o64, o32, sm, *a, s, blocks);
+        return run_ru(c, o64, o16, sm, *a, s, blocks);
     } else {
         g_last_error = "reduced-precision refinement needs degree >= 3";
         return CUTCELL_E_ARG;
@@ -350,6 +369,81 @@ const char* cutcell_last_error(void) { return g_last_error.c_str(); }
 // translation units report through cutcell_last_error.
 void cutcell_internal_set_error(const std::string& what) { g_last_error = what; }
 
+// Bounded-wait limit shared by every persistent launch of the library: 0 means
+// "not set yet" (the first read takes CUTCELL_WAIT_LIMIT_S or the default).
+static std::atomic<unsigned long long> g_wait_limit_ns{0};
+
+unsigned long long cutcell_internal_wait_limit_ns() {
+    unsigned long long v = g_wait_limit_ns.load();
+    if (v == 0) {
+        double s = CUTCELL_DEFAULT_WAIT_LIMIT_S;
+        if (const char* e = std::getenv("CUTCELL_WAIT_LIMIT_S")) {
+            const double t = std::atof(e);
+            if (t > 0.0 && t <= 3600.0) s = t;
+        }
+        unsigned long long expect = 0;
+        g_wait_limit_ns.compare_exchange_strong(expect, (unsigned long long)(s * 1e9));
+        v = g_wait_limit_ns.load();
+    }
+    return v;
+}
+
+extern "C" {
+
+int cutcell_set_wait_limit(double seconds) {
+    if (!(seconds >= 1e-3 && seconds <= 3600.0)) return CUTCELL_E_ARG;
+    g_wait_limit_ns.store((unsigned long long)(seconds * 1e9));
+    return CUTCELL_OK;
+}
+
+double cutcell_get_wait_limit(void) { return (double)cutcell_internal_wait_limit_ns() * 1e-9; }
+
+int cutcell_barrier_selftest(int32_t blocks, int32_t arrivals, int32_t* status_out) {
+    if (!status_out || blocks < 1 || arrivals < 1) return CUTCELL_E_ARG;
+    int dev = 0, sms = 0, per = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, barrier_probe_kernel, CUTCELL_BLOCK, 0));
+    if (blocks > sms * per) return CUTCELL_E_ARG;  // the grid must be co-resident
+    unsigned* bar = nullptr;
+    CK(cudaMalloc(&bar, BAR_WORDS * sizeof(unsigned)));
+    int st = CUTCELL_OK;
+    int err = 0;
+    GridSync gs;
+    gs.count = bar;
+    gs.limit_ns = cutcell_internal_wait_limit_ns();
+    gs.err = (int*)(bar + 32);
+    gs.nblocks = (unsigned)arrivals;
+    void* args[] = {(void*)&gs};
+    cudaError_t e = cudaMemset(bar, 0, BAR_WORDS * sizeof(unsigned));
+    if (e == cudaSuccess)
+        e = cudaLaunchCooperativeKernel((const void*)barrier_probe_kernel, dim3(blocks), dim3(CUTCELL_BLOCK), args, 0,
+                                        (cudaStream_t)0);
+    if (e == cudaSuccess) e = cudaMemcpy(&err, bar + 32, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) st = cuda_fail(e, "barrier self-test");
+    cudaFree(bar);
+    if (st == CUTCELL_OK) *status_out = err == 0 ? CUTCELL_OK : err;
+    return st;
+}
+
+}  // extern "C"
+
+// Validates a device CSR (sizes n, nnz) with csr_check_kernel; CUTCELL_E_SHAPE
+// if malformed.  `flag` is one device int of scratch.
+static int validate_csr(int n, int nnz, const int* ptr, const int* idx, int* flag) {
+    CK(cudaMemset(flag, 0, sizeof(int)));
+    const int blocks = std::min(ceil_div(std::max(n, nnz), 256), 1184);
+    csr_check_kernel<<<std::max(blocks, 1), 256>>>(n, nnz, ptr, idx, flag);
+    CK(cudaGetLastError());
+    int bad = 0;
+    CK(cudaMemcpy(&bad, flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (bad) {
+        g_last_error = "malformed CSR: row offsets must rise from 0 to nnz and columns lie in [0, n)";
+        return CUTCELL_E_SHAPE;
+    }
+    return CUTCELL_OK;
+}
+
 extern "C" {
 
 int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const int32_t* indices, const double* data,
@@ -360,8 +454,9 @@ int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const 
     c->n = n;
     CK(cudaGetDevice(&c->device));
     int st = alloc_scratch(c);
+    if (!st) st = validate_csr(n, nnz, indptr, indices, reinterpret_cast<int*>(c->bar));
     if (st) {
-        delete c;
+        cutcell_destroy(c);
         return st;
     }
     // threads per row from the mean row length (power of two in [1, 32])
@@ -371,12 +466,12 @@ int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const 
     c->csr64 = CsrOp<double>{n, l2, indptr, indices, data};
     if (nnz > 0) {
         CK(cudaMalloc(&c->val32, (size_t)nnz * sizeof(float)));
-        CK(cudaMalloc(&c->val16, (size_t)nnz * sizeof(__nv_bfloat16)));
+        CK(cudaMalloc(&c->val16, (size_t)nnz * sizeof(bf16x2_t)));
         to_f32_kernel<<<592, 256>>>((size_t)nnz, data, c->val32);
-        to_bf16_kernel<<<592, 256>>>((size_t)nnz, data, c->val16);
+        to_bf16x2_kernel<<<592, 256>>>((size_t)nnz, data, c->val16);
     }
     c->csr32 = CsrOp<float>{n, l2, indptr, indices, c->val32};
-    c->csr16 = CsrOp<__nv_bfloat16>{n, l2, indptr, indices, c->val16};
+    c->csr16 = CsrOp<bf16x2_t>{n, l2, indptr, indices, c->val16};
     csr_diag_inv_kernel<<<ceil_div(n, 256), 256>>>(n, indptr, indices, data, c->dinv);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
@@ -514,9 +609,9 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     }
     if (ncm) {
         CK(cudaMalloc(&c->cut32, ncm * sizeof(float)));
-        CK(cudaMalloc(&c->cut16, ncm * sizeof(__nv_bfloat16)));
+        CK(cudaMalloc(&c->cut16, ncm * sizeof(bf16x2_t)));
         to_f32_kernel<<<592, 256>>>(ncm, c->cut64, c->cut32);
-        to_bf16_kernel<<<592, 256>>>(ncm, c->cut64, c->cut16);
+        to_bf16x2_kernel<<<592, 256>>>(ncm, c->cut64, c->cut16);
     }
     ExtDev e;
     e.n_full = t->n_full;
@@ -586,11 +681,126 @@ int cutcell_pcg_create_tiles(const CutcellTileDesc* t, cutcell_ctx** out) {
     return CUTCELL_OK;
 }
 
-int cutcell_set_refinement(cutcell_ctx* c, double inner_tol, int32_t inner_maxiter, int32_t max_outer) {
-    if (!c || !(inner_tol > 0.0) || inner_maxiter < 1 || max_outer < 1) return CUTCELL_E_ARG;
-    c->inner_tol = inner_tol;
-    c->inner_maxiter = inner_maxiter;
-    c->max_outer = max_outer;
+// KronOp of a form: which = CUTCELL_FORM_* (see the header).
+static KronOp make_kron_op(cutcell_ctx* c, int which) {
+    KronOp o;
+    memset(&o, 0, sizeof(o));
+    o.nx = c->kn[0];
+    o.ny = c->kn[1];
+    o.nz = c->kn[2];
+    const size_t N = (size_t)o.nx * o.ny * o.nz;
+    o.U1 = c->kscratch;
+    o.U2 = c->kscratch + N;
+    o.V1 = c->kscratch + 2 * N;
+    o.V2 = c->kscratch + 3 * N;
+    enum { H = 0, K = 1, Q = 2, S = 3, A = 4 };
+    const KronBand(&b)[3][5] = c->kb;
+    if (which == CUTCELL_FORM_A || which == CUTCELL_FORM_K) {
+        const int f = which == CUTCELL_FORM_A ? A : K;
+        o.X0 = b[0][H];
+        o.X1 = b[0][f];
+        o.Y0 = b[1][H];
+        o.Y1 = b[1][H];
+        o.Y2 = b[1][f];
+        o.Z0 = b[2][H];
+        o.Z1 = b[2][f];
+        return o;
+    }
+    // single products: H, or Q / S on one axis and H on the others
+    int f[3] = {H, H, H};
+    if (which >= CUTCELL_FORM_QX && which <= CUTCELL_FORM_QZ) f[which - CUTCELL_FORM_QX] = Q;
+    if (which >= CUTCELL_FORM_SX && which <= CUTCELL_FORM_SZ) f[which - CUTCELL_FORM_SX] = S;
+    o.X0 = b[0][f[0]];
+    o.Y0 = b[1][f[1]];
+    o.Z1 = b[2][f[2]];
+    return o;
+}
+
+int cutcell_kron_create(const CutcellKronDesc* d, cutcell_ctx** out) {
+    if (!out || !d || !d->diag) return CUTCELL_E_ARG;
+    for (int a = 0; a < 3; ++a) {
+        if (d->n[a] < 1 || d->n[a] > 65536) return CUTCELL_E_SHAPE;
+        for (int f = 0; f < 5; ++f)
+            if (!d->factors[a][f]) return CUTCELL_E_ARG;
+    }
+    const long N = (long)d->n[0] * d->n[1] * d->n[2];
+    if (N > (1L << 30)) return CUTCELL_E_SHAPE;
+    cutcell_ctx* c = new cutcell_ctx();
+    c->kind = KIND_KRON;
+    c->n = (int)N;
+    CK(cudaGetDevice(&c->device));
+    int st = alloc_scratch(c);
+    if (st) {
+        cutcell_destroy(c);
+        return st;
+    }
+    // band form of every factor: row i's nonzeros in [lo_i, lo_i + W), the
+    // band start moved left where it would run past the last column
+    std::vector<int> lo_all;
+    std::vector<double> band_all;
+    size_t lo_off[3][5], band_off[3][5];
+    for (int a = 0; a < 3; ++a) {
+        const int n = d->n[a];
+        std::vector<double> M((size_t)n * n);
+        for (int f = 0; f < 5; ++f) {
+            CK(cudaMemcpy(M.data(), d->factors[a][f], M.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            std::vector<int> lo(n), hi(n);
+            int W = 1;
+            for (int i = 0; i < n; ++i) {
+                int l = -1, h = -1;
+                for (int j = 0; j < n; ++j)
+                    if (M[(size_t)i * n + j] != 0.0) {
+                        if (l < 0) l = j;
+                        h = j;
+                    }
+                if (l < 0) l = h = i;
+                lo[i] = l;
+                hi[i] = h;
+                W = std::max(W, h - l + 1);
+            }
+            lo_off[a][f] = lo_all.size();
+            band_off[a][f] = band_all.size();
+            for (int i = 0; i < n; ++i) {
+                const int l = std::min(lo[i], n - W);
+                lo_all.push_back(l);
+                for (int w = 0; w < W; ++w) band_all.push_back(M[(size_t)i * n + l + w]);
+            }
+            c->kb[a][f].W = W;
+        }
+        c->kn[a] = n;
+    }
+    CK(cudaMalloc(&c->klo, lo_all.size() * sizeof(int)));
+    CK(cudaMalloc(&c->kband, band_all.size() * sizeof(double)));
+    CK(cudaMemcpy(c->klo, lo_all.data(), lo_all.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->kband, band_all.data(), band_all.size() * sizeof(double), cudaMemcpyHostToDevice));
+    for (int a = 0; a < 3; ++a)
+        for (int f = 0; f < 5; ++f) {
+            c->kb[a][f].lo = c->klo + lo_off[a][f];
+            c->kb[a][f].band = c->kband + band_off[a][f];
+        }
+    CK(cudaMalloc(&c->kscratch, (size_t)4 * N * sizeof(double)));
+    diag_inv_kernel<<<ceil_div(N, 256), 256>>>((int)N, d->diag, c->dinv);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    *out = c;
+    return CUTCELL_OK;
+}
+
+int cutcell_apply_form(cutcell_ctx* c, const double* x, double* y, int32_t which, void* stream) {
+    if (!c || !x || !y || which < CUTCELL_FORM_A || which > CUTCELL_FORM_SZ) return CUTCELL_E_ARG;
+    if (c->kind == KIND_KRON) return run_apply(c, make_kron_op(c, which), 0, x, y, (cudaStream_t)stream);
+    if (which != CUTCELL_FORM_A) {
+        g_last_error = "this context holds only its SPD system form (CUTCELL_FORM_A)";
+        return CUTCELL_E_ARG;
+    }
+    return cutcell_apply(c, x, y, CUTCELL_FP64, stream);
+}
+
+int cutcell_set_refinement(cutcell_ctx* c, double replace_factor, int32_t reserved, int32_t max_replacements) {
+    if (!c || !(replace_factor > 0.0 && replace_factor < 1.0) || max_replacements < 1) return CUTCELL_E_ARG;
+    (void)reserved;
+    c->inner_tol = replace_factor;
+    c->max_outer = max_replacements;
     return CUTCELL_OK;
 }
 
@@ -601,6 +811,10 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
     if (precond < CUTCELL_PRECOND_NONE || precond > CUTCELL_PRECOND_JACOBI_LEARNED) return CUTCELL_E_ARG;
     if (precond == CUTCELL_PRECOND_JACOBI_LEARNED && (!c->mlp || precision != CUTCELL_FP64 || c->kind != KIND_TILES))
         return CUTCELL_E_ARG;
+    if (c->kind == KIND_KRON && precision != CUTCELL_FP64) {
+        g_last_error = "the Kronecker cut-box operator is solved in FP64";
+        return CUTCELL_E_ARG;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaSetDevice(c->device));
     c->use_jacobi = (precond != CUTCELL_PRECOND_NONE);
@@ -620,13 +834,15 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
     CK(cudaEventRecord(c->ev0, s));
     int blocks = 0;
     int st = CUTCELL_OK;
-    if (c->kind == KIND_CSR) {
+    if (c->kind == KIND_KRON) {
+        st = run_plain(c, make_kron_op(c, CUTCELL_FORM_A), 0, a, s, &blocks);
+    } else if (c->kind == KIND_CSR) {
         if (precision == CUTCELL_FP64)
             st = run_plain(c, c->csr64, 0, a, s, &blocks);
         else if (precision == CUTCELL_FP32_IR)
-            st = run_ir(c, c->csr64, c->csr32, 0, a, s, &blocks);
+            st = run_ru(c, c->csr64, c->csr32, 0, a, s, &blocks);
         else
-            st = run_ir(c, c->csr64, c->csr16, 0, a, s, &blocks);
+            st = run_ru(c, c->csr64, c->csr16, 0, a, s, &blocks);
     } else if (precond == CUTCELL_PRECOND_JACOBI_LEARNED) {
         st = tiles_dispatch(c, 2, precision, &a, nullptr, nullptr, s, &blocks);
     } else {
@@ -662,6 +878,8 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
 int cutcell_apply(cutcell_ctx* c, const double* x, double* y, int32_t precision, void* stream) {
     if (!c || !x || !y) return CUTCELL_E_ARG;
     cudaStream_t s = (cudaStream_t)stream;
+    if (c->kind == KIND_KRON)
+        return precision == CUTCELL_FP64 ? run_apply(c, make_kron_op(c, CUTCELL_FORM_A), 0, x, y, s) : CUTCELL_E_ARG;
     if (c->kind == KIND_CSR) {
         if (precision == CUTCELL_FP64) return run_apply(c, c->csr64, 0, x, y, s);
         if (precision == CUTCELL_FP32_IR) return run_apply(c, c->csr32, 0, x, y, s);
@@ -689,9 +907,8 @@ int cutcell_ext_scatter(cutcell_ctx* c, const double* y_full, double* y_red, voi
 
 int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
-    cudaSetDevice(c->device);
-    cudaDeviceSynchronize();
-    void* bufs[] = {c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
+    cudaSetDevice(c->device);  // cudaFree below waits for the work that may still use the buffers
+    void* bufs[] = {c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
                     c->p,     c->p2,    c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);

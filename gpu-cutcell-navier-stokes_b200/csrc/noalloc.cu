@@ -55,8 +55,11 @@ DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mu;
 thread_local std::string g_noalloc_error;
 
+// Skipped entirely when the structure check of the same call flagged the CSR
+// (the row offsets could then point anywhere).
 __global__ void noalloc_dinv_kernel(int n, const int* ptr, const int* idx, const double* val, int jacobi,
-                                    double* dinv) {
+                                    double* dinv, const int* bad) {
+    if (*((volatile const int*)bad)) return;
     for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
         double d = 0.0;
         if (jacobi)
@@ -66,9 +69,21 @@ __global__ void noalloc_dinv_kernel(int n, const int* ptr, const int* idx, const
     }
 }
 
-__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) noalloc_pcg_kernel(CsrOp<double> op, SolveArgs a) {
+__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) noalloc_pcg_kernel(CsrOp<double> op, SolveArgs a, const int* bad) {
     extern __shared__ double sm[];
     __shared__ double sh[CUTCELL_WARPS + 1];
+    // a malformed CSR (flagged by the structure check before this launch) is
+    // reported without reading it; every block sees the same flag and leaves
+    if (*((volatile const int*)bad)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            a.res->status = CUTCELL_E_SHAPE;
+            a.res->iterations = 0;
+            a.res->outer = 0;
+            a.res->rel = -1.0;
+            a.res->true_rel = -1.0;
+        }
+        return;
+    }
     int iters = 0;
     double rel = 1.0;
     int status = pcg_core(op, a.B, a.b, a.x, a.tol, a.maxiter, a.gs, sm, sh, 0.0, &iters, &rel);
@@ -95,7 +110,10 @@ int fail(cudaError_t e, const char* what) {
 // Once per device, with that device current: resolve the array's device
 // address (the host-side name is only a stand-in) and the grid size.
 int setup_device(int dev, DeviceSetup** out) {
-    if (dev < 0 || dev >= kMaxDevices) return CUTCELL_E_ARG;
+    if (dev < 0 || dev >= kMaxDevices) {
+        g_noalloc_error = "device ordinal beyond the library's fixed table of 64 devices";
+        return CUTCELL_E_ARG;
+    }
     std::lock_guard<std::mutex> lock(g_setup_mu);
     DeviceSetup& s = g_setup[dev];
     if (!s.ready) {
@@ -124,9 +142,16 @@ extern "C" {
 int cutcell_pcg_solve_csr_noalloc(int32_t n, int32_t nnz, const int32_t* indptr, const int32_t* indices,
                                   const double* data, const double* b, double* x, double tol, int32_t maxiter,
                                   int32_t precond, CutcellReport* report, void* stream) {
-    if (n <= 0 || nnz < 0 || !indptr || (nnz > 0 && (!indices || !data)) || !b || !x || maxiter < 0 || !(tol >= 0.0))
+    g_noalloc_error.clear();
+    if (n <= 0 || nnz < 0 || !indptr || (nnz > 0 && (!indices || !data)) || !b || !x || maxiter < 0 ||
+        !(tol >= 0.0)) {
+        g_noalloc_error = "invalid argument: n > 0, nnz >= 0, non-null arrays, maxiter >= 0 and tol >= 0 are required";
         return CUTCELL_E_ARG;
-    if (precond != CUTCELL_PRECOND_NONE && precond != CUTCELL_PRECOND_JACOBI) return CUTCELL_E_ARG;
+    }
+    if (precond != CUTCELL_PRECOND_NONE && precond != CUTCELL_PRECOND_JACOBI) {
+        g_noalloc_error = "invalid argument: precond must be CUTCELL_PRECOND_NONE or CUTCELL_PRECOND_JACOBI";
+        return CUTCELL_E_ARG;
+    }
     if (n > CUTCELL_NOALLOC_MAX_N) {
         g_noalloc_error = "n exceeds the fixed scratch (CUTCELL_NOALLOC_MAX_N unknowns)";
         return CUTCELL_E_SHAPE;
@@ -140,11 +165,15 @@ int cutcell_pcg_solve_csr_noalloc(int32_t n, int32_t nnz, const int32_t* indptr,
     cudaStream_t s = (cudaStream_t)stream;
     double* base = S->base;
     unsigned* ctrl = reinterpret_cast<unsigned*>(base + kOffCtrl);
-    // words that must start at zero: barrier arrival and error words
+    // words that must start at zero: barrier arrival, error and CSR-check words
     if ((e = cudaMemsetAsync(ctrl, 0, CUTCELL_NOALLOC_CTRL_WORDS * sizeof(unsigned), s)) != cudaSuccess)
         return fail(e, "cudaMemsetAsync");
+    int* bad = reinterpret_cast<int*>(ctrl + 64);
+    csr_check_kernel<<<ceil_div(n > nnz ? n : nnz, 256) < 1184 ? ceil_div(n > nnz ? n : nnz, 256) : 1184, 256, 0, s>>>(
+        n, nnz, indptr, indices, bad);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "csr_check_kernel launch");
     noalloc_dinv_kernel<<<ceil_div(n, 256), 256, 0, s>>>(n, indptr, indices, data,
-                                                        precond == CUTCELL_PRECOND_JACOBI, base + kOffDinv);
+                                                        precond == CUTCELL_PRECOND_JACOBI, base + kOffDinv, bad);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "noalloc_dinv_kernel launch");
     const double mean = nnz / (double)n;
     int l2 = 0;
@@ -158,7 +187,7 @@ int cutcell_pcg_solve_csr_noalloc(int32_t n, int32_t nnz, const int32_t* indptr,
     a.maxiter = maxiter;
     a.res = reinterpret_cast<DevResult*>(base + kOffRes);
     a.gs.count = ctrl;
-    a.gs.gen = ctrl;
+    a.gs.limit_ns = cutcell_internal_wait_limit_ns();
     a.gs.err = reinterpret_cast<int*>(ctrl + 32);
     a.gs.nblocks = (unsigned)S->blocks;
     a.B.n = n;
@@ -167,7 +196,8 @@ int cutcell_pcg_solve_csr_noalloc(int32_t n, int32_t nnz, const int32_t* indptr,
     a.B.p = base + kOffP;
     a.B.Ap = base + kOffAp;
     a.B.part = base + kOffPart;
-    void* args[] = {(void*)&op, (void*)&a};
+    const int* badc = bad;
+    void* args[] = {(void*)&op, (void*)&a, (void*)&badc};
     e = cudaLaunchCooperativeKernel((const void*)noalloc_pcg_kernel, dim3(S->blocks), dim3(CUTCELL_BLOCK), args, 0, s);
     if (e != cudaSuccess) return fail(e, "cudaLaunchCooperativeKernel");
     DevResult hr;
@@ -183,7 +213,15 @@ int cutcell_pcg_solve_csr_noalloc(int32_t n, int32_t nnz, const int32_t* indptr,
         report->true_relative_residual = hr.true_rel;
         report->elapsed_ms = 0.0;  // not timed: no events are created on this path
     }
-    return hr.status == CUTCELL_E_BARRIER ? CUTCELL_E_BARRIER : CUTCELL_OK;
+    if (hr.status == CUTCELL_E_SHAPE) {
+        g_noalloc_error = "malformed CSR: row offsets must rise from 0 to nnz and columns lie in [0, n)";
+        return CUTCELL_E_SHAPE;
+    }
+    if (hr.status == CUTCELL_E_BARRIER) {
+        g_noalloc_error = "a device-wide wait ran out (cutcell_set_wait_limit)";
+        return CUTCELL_E_BARRIER;
+    }
+    return CUTCELL_OK;
 }
 
 const char* cutcell_noalloc_last_error(void) { return g_noalloc_error.c_str(); }

@@ -58,6 +58,22 @@ struct CsrOp {
     }
 };
 
+// CSR structure check: row offsets start at 0, end at nnz and never decrease;
+// every column index lies in [0, n).  Reads only ptr[0..n] and idx[0..nnz), so
+// it is safe on any input of the stated sizes; *bad receives 1 on a violation.
+static __global__ void csr_check_kernel(int n, int nnz, const int* ptr, const int* idx, int* bad) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+    int b = 0;
+    if (gtid == 0 && (ptr[0] != 0 || ptr[n] != nnz)) b = 1;
+    for (int i = gtid; i < n; i += gs)
+        if (ptr[i + 1] < ptr[i]) b = 1;
+    for (int k = gtid; k < nnz; k += gs) {
+        const int j = idx[k];
+        if (j < 0 || j >= n) b = 1;
+    }
+    if (b) atomicExch(bad, 1);
+}
+
 // ---------------------------------------------------------------------------
 // Aggregation extension E (n_full x n_red): identity rows + small rows.
 // ---------------------------------------------------------------------------

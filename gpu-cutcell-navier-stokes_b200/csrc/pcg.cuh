@@ -1,5 +1,5 @@
-// Persistent Jacobi-PCG and FP64 iterative refinement, one cooperative launch
-// per solve.  The iteration is the one of solve_gpu_cg
+// Persistent Jacobi-PCG and its reduced-precision form with FP64 residual
+// replacement, one cooperative launch per solve.  The iteration is the one of solve_gpu_cg
 // (code/fast_solver_backends.py:236-274):
 //
 //   x = 0, r = b, z = D^{-1} r (z = r where the diagonal is zero), p = z
@@ -170,12 +170,12 @@ struct SolveArgs {
     double* x;
     double tol;
     int maxiter;
-    // refinement
-    double inner_tol;
-    int inner_maxiter;
-    int max_outer;
-    double* d;      // correction
-    double* rhat;   // outer residual
+    // reduced-precision forms
+    double inner_tol;   // residual-replacement factor (ru_kernel)
+    int inner_maxiter;  // unused
+    int max_outer;      // replacement cap (ru_kernel)
+    double* d;          // scratch vector
+    double* rhat;       // scratch vector
     GridSync gs;
     PcgBufs B;
     DevResult* res;
@@ -204,90 +204,168 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) pcg_kernel(Op op, SolveArgs 
     }
 }
 
-// FP64 iterative refinement around a reduced-precision inner PCG:
-//   x = 0; rhat = b
-//   repeat: solve A_lo d = rhat (PCG, relative tolerance inner_tol);
-//           x += d; rhat = b - A_64 x (FP64); stop when ||rhat||/||b|| <= tol.
+// Reduced-precision PCG with FP64 residual replacement ("reliable updates",
+// the refinement form of the FP32 / BF16 operators).  It is the Jacobi-PCG of
+// pcg_core with A p evaluated by the reduced-precision operator `lo`; the
+// iterate, the residual, the search direction and every dot product stay in
+// FP64.  The recursive residual drifts from the true one by the operator's
+// rounding, so it is replaced by the FP64 true residual b - A x (operator `hi`)
+// whenever its norm has fallen by `replace` below the largest norm since the
+// last replacement, and whenever the recursive test says converged.  The
+// search direction is kept across a replacement, so the Krylov space is not
+// restarted (a restarted refinement re-grows it every sweep).  Success needs
+// the TRUE residual <= tol, or, once the recursive test has passed and the
+// true residual has stopped halving (the FP64 attainable-accuracy floor), the
+// reference's success bound true <= max(10 tol, 1e-14).  A run of
+// replacements whose true residuals do not halve otherwise means the reduced
+// operator cannot resolve the remaining error: the solve stops with
+// CUTCELL_E_NOCONV instead of spinning to maxiter.
+//   iterations: total PCG iterations (each one reduced-precision apply);
+//   outer: replacements made + 1.
 template <class OpHi, class OpLo>
-__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) ir_kernel(OpHi hi, OpLo lo, SolveArgs a) {
+__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) ru_kernel(OpHi hi, OpLo lo, SolveArgs a) {
     extern __shared__ double sm[];
     __shared__ double sh[CUTCELL_WARPS + 1];
-    const int n = a.B.n;
+    const PcgBufs& B = a.B;
+    const int n = B.n;
+    const int nb = gridDim.x;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
-#ifdef CUTCELL_DEBUG_CHECKS
-    if (threadIdx.x == 0) {
-        unsigned* w = a.gs.count + 128;
-        CUTCELL_OK_IF(CUTCELL_ALIGNED(a.x, 8) && CUTCELL_ALIGNED(a.b, 8) && CUTCELL_ALIGNED(a.d, 8) &&
-                          CUTCELL_ALIGNED(a.rhat, 8),
-                      20, 0, w);
-        CUTCELL_OK_IF(CUTCELL_ALIGNED(a.B.r, 8) && CUTCELL_ALIGNED(a.B.p, 8) && CUTCELL_ALIGNED(a.B.Ap, 8) &&
-                          CUTCELL_ALIGNED(a.B.dinv, 8) && CUTCELL_ALIGNED(a.B.part, 8),
-                      21, 0, w);
-        CUTCELL_OK_IF(CUTCELL_ALIGNED(a.res, 8) && CUTCELL_ALIGNED(a.gs.count, 4) && CUTCELL_ALIGNED(a.gs.err, 4), 22, 0,
-                      w);
-        CUTCELL_OK_IF(CUTCELL_ALIGNED(sm, 16) && CUTCELL_ALIGNED(sh, 8), 23, 0, w);
-    }
-#endif
+    double* part = B.part;
+    double* x = a.x;
+    double rz_p = 0.0, bb_p = 0.0;
     for (int i = gtid; i < n; i += gstride) {
-        a.x[i] = 0.0;
-        a.rhat[i] = a.b[i];
+        const double bi = a.b[i];
+        x[i] = 0.0;
+        B.r[i] = bi;
+        const double zi = B.dinv[i] * bi;
+        B.p[i] = zi;
+        rz_p += bi * zi;
+        bb_p += bi * bi;
     }
-    double bn = norm_of(a.b, n, a.B.part, a.gs, sh, 6);
-    if (bn == 0.0) bn = 1.0;
-    int total = 0, outer = 0;
+    rz_p = block_sum(rz_p, sh);
+    bb_p = block_sum(bb_p, sh);
+    if (threadIdx.x == 0) {
+        part[0 * nb + blockIdx.x] = rz_p;
+        part[1 * nb + blockIdx.x] = bb_p;
+    }
     int status = CUTCELL_E_NOCONV;
-    double true_rel = 1.0, rel_in = 1.0, prev = 1.0;
-    int stall = 0;
-    for (outer = 1; outer <= a.max_outer; ++outer) {
-        int it = 0;
-        const int budget = a.maxiter - total;
-        if (budget <= 0) break;
-        // the inner solve may not grow its residual by more than 1e3: a
-        // reduced-precision operator that lost definiteness stops the sweep
-        int st = pcg_core(lo, a.B, a.rhat, a.d, a.inner_tol, budget < a.inner_maxiter ? budget : a.inner_maxiter,
-                          a.gs, sm, sh, 1.0e3, &it, &rel_in);
-        total += it;
-        if (st == CUTCELL_E_BARRIER) {
-            status = st;
-            break;
-        }
-        if (st == CUTCELL_E_NAN || (st == CUTCELL_E_BREAKDOWN && it <= 1)) {
-            status = CUTCELL_E_BREAKDOWN;  // correction discarded, x keeps the last refined iterate
-            break;
-        }
-        for (int i = gtid; i < n; i += gstride) a.x[i] += a.d[i];
-        if (!grid_sync(a.gs)) {
-            status = CUTCELL_E_BARRIER;
-            break;
-        }
-        true_rel = true_residual(hi, a.B, a.b, a.x, bn, a.gs, sm, sh, a.rhat);
-        if (grid_error(a.gs)) {
-            status = CUTCELL_E_BARRIER;
-            break;
-        }
-        if (!isfinite(true_rel)) {
-            status = CUTCELL_E_NAN;
-            break;
-        }
-        if (true_rel <= a.tol) {
-            status = CUTCELL_OK;
-            break;
-        }
-        // stagnation: two sweeps in a row that do not halve the true residual
-        stall = (true_rel > 0.5 * prev) ? stall + 1 : 0;
-        prev = true_rel;
-        if (stall >= 2) {
-            status = CUTCELL_E_NOCONV;
-            break;
+    int k = 0, nrep = 0, stall = 0;
+    double rel = 1.0, true_rel = 1.0, last_true = 1.0;
+    if (grid_sync(a.gs)) {
+        double rz = grid_reduce(part + 0 * nb, nb, sh);
+        double bnorm = sqrt(grid_reduce(part + 1 * nb, nb, sh));
+        if (bnorm == 0.0) bnorm = 1.0;
+        double rmax = bnorm * rel;
+        double* P[2] = {B.p, OpLo::kFusedP ? B.p2 : B.p};
+        double beta = 0.0;
+        for (k = 1; k <= a.maxiter; ++k) {
+            double* pk = P[(k - 1) & 1];
+            double pap;
+            if constexpr (OpLo::kFusedP) {
+                pap = (k > 1) ? lo.apply_next(P[k & 1], pk, B.r, B.dinv, beta, B.Ap, a.gs, sm) : lo.apply(pk, B.Ap, a.gs, sm);
+            } else {
+                pap = lo.apply(pk, B.Ap, a.gs, sm);
+            }
+            if (grid_error(a.gs)) break;
+            pap = block_sum(pap, sh);
+            if (threadIdx.x == 0) part[2 * nb + blockIdx.x] = pap;
+            if (!grid_sync(a.gs)) break;
+            pap = grid_reduce(part + 2 * nb, nb, sh);
+            if (!(pap > 0.0) || !isfinite(pap)) {
+                status = CUTCELL_E_BREAKDOWN;
+                break;
+            }
+            const double alpha = rz / pap;
+            double rr_p = 0.0, rzn_p = 0.0;
+            for (int i = gtid; i < n; i += gstride) {
+                const double pi = __ldcg(pk + i);
+                x[i] += alpha * pi;
+                const double ri = B.r[i] - alpha * __ldcg(B.Ap + i);
+                B.r[i] = ri;
+                rr_p += ri * ri;
+                rzn_p += ri * (B.dinv[i] * ri);
+            }
+            rr_p = block_sum(rr_p, sh);
+            rzn_p = block_sum(rzn_p, sh);
+            if (threadIdx.x == 0) {
+                part[3 * nb + blockIdx.x] = rr_p;
+                part[4 * nb + blockIdx.x] = rzn_p;
+            }
+            if (!grid_sync(a.gs)) break;
+            double rn = sqrt(grid_reduce(part + 3 * nb, nb, sh));
+            double rzn = grid_reduce(part + 4 * nb, nb, sh);
+            rel = rn / bnorm;
+            if (!isfinite(rel)) {
+                status = CUTCELL_E_NAN;
+                break;
+            }
+            rmax = rn > rmax ? rn : rmax;
+            const bool by_test = rel <= a.tol;
+            if (by_test || rn < a.inner_tol * rmax) {
+                // replacement: r = b - A_64 x in FP64, and its dots
+                hi.apply(x, B.Ap, a.gs, sm);
+                if (!grid_sync(a.gs)) break;
+                double t_p = 0.0, tz_p = 0.0;
+                for (int i = gtid; i < n; i += gstride) {
+                    const double ri = a.b[i] - __ldcg(B.Ap + i);
+                    B.r[i] = ri;
+                    t_p += ri * ri;
+                    tz_p += ri * (B.dinv[i] * ri);
+                }
+                t_p = block_sum(t_p, sh);
+                tz_p = block_sum(tz_p, sh);
+                if (threadIdx.x == 0) {
+                    part[5 * nb + blockIdx.x] = t_p;
+                    part[6 * nb + blockIdx.x] = tz_p;
+                }
+                if (!grid_sync(a.gs)) break;
+                rn = sqrt(grid_reduce(part + 5 * nb, nb, sh));
+                rzn = grid_reduce(part + 6 * nb, nb, sh);
+                ++nrep;
+                true_rel = rn / bnorm;
+                rel = true_rel;
+                rmax = rn;
+                if (!isfinite(true_rel)) {
+                    status = CUTCELL_E_NAN;
+                    break;
+                }
+                if (true_rel <= a.tol) {
+                    status = CUTCELL_OK;
+                    break;
+                }
+                // at the FP64 attainable-accuracy floor: the recursive test
+                // passed, the true residual meets the reference's success
+                // bound max(10 tol, 1e-14) (code/fast_solver_backends.py:283)
+                // and no longer halves between replacements
+                const double floor_ok = fmax(10.0 * a.tol, 1e-14);
+                if (by_test && true_rel <= floor_ok && true_rel > 0.5 * last_true) {
+                    status = CUTCELL_OK;
+                    break;
+                }
+                // the reduced operator no longer resolves the error
+                stall = (true_rel > 0.5 * last_true) ? stall + 1 : 0;
+                last_true = true_rel;
+                if (stall >= 3 || nrep >= a.max_outer) {
+                    status = CUTCELL_E_NOCONV;
+                    break;
+                }
+            }
+            beta = rzn / rz;
+            rz = rzn;
+            if constexpr (!OpLo::kFusedP) {
+                for (int i = gtid; i < n; i += gstride) B.p[i] = p_next(B.dinv[i], B.r[i], beta, B.p[i]);
+                if (!grid_sync(a.gs)) break;
+            }
         }
     }
+    if (grid_error(a.gs)) status = CUTCELL_E_BARRIER;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.res->status = status;
-        a.res->iterations = total;
-        a.res->outer = outer > a.max_outer ? a.max_outer : outer;
-        a.res->rel = true_rel;
-        a.res->true_rel = true_rel;
+        a.res->iterations = k > a.maxiter ? a.maxiter : k;
+        a.res->outer = nrep + 1;
+        a.res->rel = rel;
+        a.res->true_rel = nrep > 0 ? true_rel : -1.0;
     }
 }
 

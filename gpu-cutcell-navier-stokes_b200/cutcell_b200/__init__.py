@@ -7,6 +7,6 @@ aggregation ``E`` (``aggregation``), the tile layout and device operator
 loaded through ``_lib`` (C ABI in include/cutcell_b200.h).
 """
 
-from .fast_solver_backends import SolverReport, as_csr, csr_memory_bytes, solve_spd  # noqa: F401
+from .fast_solver_backends import SolverReport, as_csr, csr_memory_bytes, make_linear_solver, solve_spd  # noqa: F401
 
-__all__ = ["SolverReport", "as_csr", "csr_memory_bytes", "solve_spd"]
+__all__ = ["SolverReport", "as_csr", "csr_memory_bytes", "make_linear_solver", "solve_spd"]

@@ -157,6 +157,11 @@ SIGNATURES = {
         [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, C.c_double, C.c_int32, C.c_int32, C.POINTER(CutcellReport), _P],
     ),
     "cutcell_noalloc_last_error": (C.c_char_p, []),
+    "cutcell_set_wait_limit": (C.c_int, [C.c_double]),
+    "cutcell_kron_create": (C.c_int, [_P, C.POINTER(_P)]),
+    "cutcell_apply_form": (C.c_int, [_P, _P, _P, C.c_int32, _P]),
+    "cutcell_get_wait_limit": (C.c_double, []),
+    "cutcell_barrier_selftest": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "cutcell_status_string": (C.c_char_p, [C.c_int]),
     "cutcell_last_error": (C.c_char_p, []),
 }

@@ -93,8 +93,12 @@ class CsrDeviceMatrix:
             )
         self._ctx = ctx
 
-    def set_refinement(self, inner_tol: float, inner_maxiter: int = 100000, max_outer: int = 50) -> None:
-        _lib.check(self._lib.cutcell_set_refinement(self._ctx, float(inner_tol), int(inner_maxiter), int(max_outer)), "refinement")
+    def set_refinement(self, replace_factor: float = 0.1, max_replacements: int = 200) -> None:
+        """Controls of the FP32 / BF16 forms (PCG with the reduced-precision
+        operator and FP64 residual replacement): the recursive residual is
+        replaced by the FP64 true residual each time its norm falls by
+        ``replace_factor``; at most ``max_replacements`` replacements."""
+        _lib.check(self._lib.cutcell_set_refinement(self._ctx, float(replace_factor), 0, int(max_replacements)), "refinement")
 
     def apply(self, x, precision: str = "fp64"):
         import torch
@@ -165,7 +169,7 @@ def solve_b200_cg(
     maxiter: int = 5000,
     preconditioner: Preconditioner = "jacobi",
     precision: Precision = "fp64",
-    inner_tol: float | None = None,
+    replace_factor: float = 0.1,
     device="cuda",
 ) -> tuple[np.ndarray | None, SolverReport]:
     """Jacobi-PCG on the B200, host arrays in and out (the solve_gpu_cg contract)."""
@@ -191,7 +195,7 @@ def solve_b200_cg(
     torch.cuda.synchronize(dev_op.device)
     transfer = perf_counter() - t0
     if precision != "fp64":
-        dev_op.set_refinement(inner_tol if inner_tol is not None else (1e-2 if precision == "bf16-ir" else 1e-4))
+        dev_op.set_refinement(replace_factor)
     tic = perf_counter()
     x_dev, rep = dev_op.solve_device(b_dev, tol=tol, maxiter=maxiter, precision=precision, preconditioner=preconditioner)
     x = x_dev.cpu().numpy()
@@ -226,3 +230,22 @@ def solve_spd(
 
         return solve_learned(A, b, tol=tol, maxiter=maxiter, precision=precision, **kw)
     return solve_b200_cg(A, b, tol=tol, maxiter=maxiter, preconditioner=preconditioner, precision=precision, **kw)
+
+
+def make_linear_solver(*, backend: Backend = "b200", tol: float = 1.0e-13, maxiter: int = 20000,
+                       preconditioner: Preconditioner = "jacobi", precision: Precision = "fp64"):
+    """A ``linear_solver(A, b) -> x`` callable that routes a wrapper's dense
+    ``np.linalg.solve(A, b)`` through ``solve_spd`` (the opt-in
+    ``linear_solver=`` of code/cut_3d_sbp.py:503 and
+    code/cut_pde_solve.py:446).  A may be dense or sparse and must be SPD; the
+    call raises ``RuntimeError`` with the solver's message when the solve does
+    not succeed, since those wrappers have no failure path of their own."""
+
+    def linear_solver(A, b):
+        x, rep = solve_spd(A, np.asarray(b, dtype=float), backend=backend, tol=tol, maxiter=maxiter,
+                           preconditioner=preconditioner, precision=precision)
+        if x is None or not rep.success:
+            raise RuntimeError(f"linear_solver: {rep.message} (relative residual {rep.relative_residual:.2e})")
+        return x
+
+    return linear_solver

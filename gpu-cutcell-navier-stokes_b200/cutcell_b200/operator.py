@@ -258,9 +258,13 @@ class CutCellOperator:
     def reduced_load(self) -> np.ndarray:
         return np.asarray(self.extension.E.T @ self.problem.load)
 
-    def set_refinement(self, inner_tol: float, inner_maxiter: int = 100000, max_outer: int = 50) -> None:
+    def set_refinement(self, replace_factor: float = 0.1, max_replacements: int = 200) -> None:
+        """Controls of the FP32 / BF16 forms (PCG with the reduced-precision
+        operator and FP64 residual replacement): the recursive residual is
+        replaced by the FP64 true residual each time its norm falls by
+        ``replace_factor``; at most ``max_replacements`` replacements."""
         _lib.check(
-            self._lib.cutcell_set_refinement(self._ctx, float(inner_tol), int(inner_maxiter), int(max_outer)),
+            self._lib.cutcell_set_refinement(self._ctx, float(replace_factor), 0, int(max_replacements)),
             "cutcell_set_refinement",
         )
 

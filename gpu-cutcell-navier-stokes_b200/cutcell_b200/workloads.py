@@ -101,6 +101,27 @@ def sliver_plane(n: int, normal, fraction: float) -> PlaneLevelSet:
     return PlaneLevelSet(tuple(nrm), 0.5 * (lo + hi) / n)
 
 
+def sliver_stress_cases(count: int = 25, seed: int = 20260629):
+    """The mixed-precision sliver stress set: ``count`` planar cuts of the unit
+    box with normals |g| / ||g||, g ~ N(0, I_3) (uniform on the positive
+    octant), and worst cut-cell fluid fractions 10^U(-5, -1) (log-uniform in
+    [1e-5, 1e-1]); seeded.  Returns [(normal, fraction)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        g = np.abs(rng.standard_normal(3))
+        g = np.maximum(g, 1e-3)  # strictly inside the octant
+        eps = float(10.0 ** rng.uniform(-5.0, -1.0))
+        out.append((g / np.linalg.norm(g), eps))
+    return out
+
+
+def stress_rhs(n_reduced: int, n_elements: int, degree: int) -> np.ndarray:
+    """N(0, 1) right-hand side with the seed rule of the reference's stress
+    driver (code/fast_solver_workbench.py:167): 12345 + 17 n + p."""
+    return np.random.default_rng(12345 + 17 * n_elements + degree).standard_normal(n_reduced)
+
+
 def plane_offset_for_fraction(n: int, angle_deg: float, fraction: float) -> float:
     """Offset of the plane n.x = c such that the smallest nonzero cut-cell
     fluid fraction equals ``fraction`` (bisection on the exact polyhedral

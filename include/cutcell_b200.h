@@ -107,7 +107,10 @@ typedef struct {
 
 /* Replaces the CuPy CSR upload + Jacobi-CG loop of solve_gpu_cg
  * (code/fast_solver_backends.py:194-289): CSR of the reduced SPD matrix
- * (int32 indptr/indices, fp64 data), already on the device. */
+ * (int32 indptr/indices, fp64 data), already on the device.  The structure is
+ * checked on the device at create (indptr[0] = 0, indptr[n] = nnz, indptr
+ * non-decreasing, every column in [0, n)); a malformed matrix returns
+ * CUTCELL_E_SHAPE and no context. */
 int cutcell_pcg_create_csr(int32_t n, int32_t nnz, const int32_t* indptr, const int32_t* indices,
                            const double* data, cutcell_ctx** out);
 
@@ -131,6 +134,41 @@ int cutcell_pcg_solve(cutcell_ctx* ctx, const double* b, double* x, double tol, 
 
 /* y = E^T A E x (reduced vectors), operator data in the given precision. */
 int cutcell_apply(cutcell_ctx* ctx, const double* x, double* y, int32_t precision, void* stream);
+
+/* ---- tensor-product cut boxes (assemble_cut_3d / solve_poisson_3d,
+ * code/cut_3d_sbp.py:89-146,386-503) ----
+ * All their forms are sums of Kronecker products of reduced 1D factors
+ * E_a^T C_a E_a (E = Ez (x) Ey (x) Ex), applied matrix-free by three
+ * sum-factorised passes; no N x N matrix is formed.  create: the reduced 1D
+ * sizes n[a] (x, y, z) and per axis the dense row-major factors (device, n_a x
+ * n_a, copied into a banded form at create) of the mass H, stiffness K,
+ * advection Q (Q_ij = int phi_i phi_j'), boundary form S, and the weak-penalty
+ * Poisson factor A = K + beta (tL tL^T + tR tR^T) - N - N^T
+ * (N = tL (-dL)^T + tR dR^T); diag: the diagonal of the 3D Poisson form
+ * (Jacobi).  The context solves (cutcell_pcg_solve, FP64, precond NONE or
+ * JACOBI) the Poisson system
+ *   A3 = Hz (x) Hy (x) Ax + Hz (x) Ay (x) Hx + Az (x) Hy (x) Hx,
+ * and applies every form through cutcell_apply_form. */
+enum {
+    CUTCELL_FORM_A = 0,  /* the context's SPD system (all context kinds) */
+    CUTCELL_FORM_H = 1,  /* Hz (x) Hy (x) Hx */
+    CUTCELL_FORM_K = 2,  /* Hz Hy Kx + Hz Ky Hx + Kz Hy Hx */
+    CUTCELL_FORM_QX = 3, /* Hz (x) Hy (x) Qx */
+    CUTCELL_FORM_QY = 4,
+    CUTCELL_FORM_QZ = 5,
+    CUTCELL_FORM_SX = 6, /* Hz (x) Hy (x) Sx */
+    CUTCELL_FORM_SY = 7,
+    CUTCELL_FORM_SZ = 8
+};
+typedef struct {
+    int32_t n[3];
+    const double* factors[3][5]; /* [axis x, y, z][H, K, Q, S, A] */
+    const double* diag;
+} CutcellKronDesc;
+int cutcell_kron_create(const CutcellKronDesc* desc, cutcell_ctx** out);
+/* y = F x for a form F of the context (CUTCELL_FORM_*, FP64); CSR and tile
+ * contexts hold only CUTCELL_FORM_A. */
+int cutcell_apply_form(cutcell_ctx* ctx, const double* x, double* y, int32_t which, void* stream);
 
 /* Extension gather x_full = E x_red and transpose scatter y_red = E^T y_full
  * (E as produced by polynomial_preserving_extension_3d,
@@ -291,11 +329,33 @@ int cutcell_batch_destroy(cutcell_batch* batch);
  * first call on each device resolves the array's address and the grid size;
  * make that first call before any stream capture.  Calls share the array:
  * calls that overlap on the GPU race and must be serialised by the caller.
- * report->elapsed_ms is 0 (no events are created on this path). */
+ * The CSR structure is checked on the device first (as in
+ * cutcell_pcg_create_csr); a malformed matrix returns CUTCELL_E_SHAPE
+ * without being read further.  Solver outcomes (maximum iterations reached,
+ * breakdown, non-finite residual) are reported in report->status, as with
+ * cutcell_pcg_solve, and the call returns CUTCELL_OK for them; pass a report
+ * to see them.  The call waits for its stream before it returns.
+ * report->elapsed_ms is 0 (no events are created on this path).
+ * cutcell_noalloc_last_error: the message of this thread's last failed call
+ * (empty after a call that returned CUTCELL_OK). */
 int cutcell_pcg_solve_csr_noalloc(int32_t n, int32_t nnz, const int32_t* indptr, const int32_t* indices,
                                   const double* data, const double* b, double* x, double tol, int32_t maxiter,
                                   int32_t precond, CutcellReport* report, void* stream);
 const char* cutcell_noalloc_last_error(void);
+
+/* Bounded waits.  Every device-wide wait of the persistent kernels (grid
+ * barriers) gives up after a limit of global-timer (wall-clock) time, sets
+ * CUTCELL_E_BARRIER and returns, leaving the context usable.  The limit is
+ * process-wide: 10 s by default, or CUTCELL_WAIT_LIMIT_S from the environment
+ * at the first launch; set_wait_limit takes seconds in [1e-3, 3600].
+ * barrier_selftest runs one grid barrier over `blocks` co-resident blocks that
+ * waits for `arrivals` arrivals on the current device and stream 0, and
+ * stores the device's status: CUTCELL_OK when arrivals <= blocks, and
+ * CUTCELL_E_BARRIER after the limit when arrivals > blocks (nothing ever
+ * completes that barrier).  No counterpart in the reference (diagnostics). */
+int cutcell_set_wait_limit(double seconds);
+double cutcell_get_wait_limit(void);
+int cutcell_barrier_selftest(int32_t blocks, int32_t arrivals, int32_t* status_out);
 
 int cutcell_destroy(cutcell_ctx* ctx);
 const char* cutcell_status_string(int status);

@@ -3,20 +3,30 @@ oracle/_ref/hill_ref (test infrastructure; outputs only under oracle/_ref/).
 
 The reference path is header-only C++17 (cpp/include/{core,cut,...}), so it
 is compiled directly from its sources where they lie -- no reference build
-system is run.  Needs the reference tree (default /root/reference).
+system is run.  Needs the reference tree: an explicit argument, else the
+environment variable CUTCELL_REFERENCE_ROOT, else the checkout location this
+recipe was written for (READ_ONLY_CHECKOUT).  Every script that reads the
+reference resolves its location through ``reference_root``.
 """
 
 from __future__ import annotations
 
+import os
 import subprocess
 import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
+READ_ONLY_CHECKOUT = "/root/reference"
 
 
-def build(ref_root: str = "/root/reference") -> Path | None:
-    inc = Path(ref_root) / "cpp" / "include"
+def reference_root(arg: str | None = None) -> Path:
+    """Location of the reference tree (argument > CUTCELL_REFERENCE_ROOT > checkout)."""
+    return Path(arg or os.environ.get("CUTCELL_REFERENCE_ROOT") or READ_ONLY_CHECKOUT)
+
+
+def build(ref_root: str | None = None) -> Path | None:
+    inc = reference_root(ref_root) / "cpp" / "include"
     if not inc.exists():
         return None
     out = HERE / "_ref" / "hill_ref"

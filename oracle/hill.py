@@ -167,7 +167,7 @@ def read_reference_dump(path):
     return d
 
 
-def reference_dump(ne=3, nz=6, seed=99, steps=1, ref_root="/root/reference"):
+def reference_dump(ne=3, nz=6, seed=99, steps=1, ref_root=None):
     """Run the compiled reference (oracle/_ref/hill_ref; built from the
     reference's headers when the tree is present) and parse its dump.
     Returns None when the binary is unavailable."""

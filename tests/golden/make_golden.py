@@ -118,4 +118,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+    from oracle.build_ref import reference_root
+
+    main(str(reference_root(sys.argv[1] if len(sys.argv) > 1 else None)))

@@ -22,7 +22,7 @@ REPO = HERE.parents[1]
 sys.path.insert(0, str(REPO))
 
 
-def main(ref_root="/root/reference", ne=6, nz=12, seed=99, steps=1):
+def main(ref_root=None, ne=6, nz=12, seed=99, steps=1):
     from oracle.build_ref import build
 
     exe = build(ref_root)

@@ -48,3 +48,14 @@ def test_report_fields_superset_of_reference():
     names = [f.name for f in fields(SolverReport)]
     ref = ["backend", "method", "preconditioner", "success", "iterations", "elapsed_s", "relative_residual", "message", "transfer_s"]
     assert names[: len(ref)] == ref
+
+
+def test_wait_limit_setter_validates_and_round_trips():
+    lib = _lib.load()
+    old = lib.cutcell_get_wait_limit()
+    assert 1e-3 <= old <= 3600.0
+    assert lib.cutcell_set_wait_limit(0.0) == _lib.E_ARG
+    assert lib.cutcell_set_wait_limit(1e9) == _lib.E_ARG
+    assert lib.cutcell_set_wait_limit(2.5) == _lib.OK
+    assert abs(lib.cutcell_get_wait_limit() - 2.5) < 1e-9
+    assert lib.cutcell_set_wait_limit(old) == _lib.OK

@@ -1,15 +1,19 @@
-"""Mixed precision under sliver stress: 3D plane-cut boxes, p = 4, n = 16
-(8,000 full DOFs), normals |g| / ||g|| with g ~ N(0, I) on the positive
-octant, worst cut-cell fluid fraction 1e-5 .. 1e-1, N(0, 1) right-hand
-sides (seed 12345).  FP64 matrix-free Jacobi-PCG against the oracle's CG on
-the assembled E^T A E; FP32 / BF16 operator storage inside FP64 iterative
-refinement against the FP64 solution.
+"""Mixed precision under sliver stress (the 25-cut set): 3D plane-cut boxes,
+p = 4, n = 16 (8,000 full DOFs), normals |g| / ||g|| with g ~ N(0, I) on the
+positive octant and worst cut-cell fluid fractions log-uniform in
+[1e-5, 1e-1] (workloads.sliver_stress_cases, seeded), N(0, 1) right-hand
+sides with the reference stress driver's seed rule 12345 + 17 n + p
+(code/fast_solver_workbench.py:167).
 
-Bars: at tol 1e-9 the FP64 iterations are within max(1, 2 %) of the
-oracle's; solved to tol 1e-13, the FP64 solution is within 1e-9 (relative
-L2) of the oracle's 1e-13 solution and the FP32 refinement within 1e-7;
-BF16 refinement either meets the FP32 bar at tol 1e-9 or stops cleanly
-(breakdown or stagnation, finite iterate)."""
+Every case, on the device: FP64 matrix-free Jacobi-PCG converges at tol 1e-9
+and 1e-13; the FP32 and BF16 operator forms (PCG with FP64 residual
+replacement) converge at tol 1e-9 with iteration counts within the stated
+factor of plain FP64's, and solved to tol 1e-11 they lie within 1e-7
+(relative L2) of the FP64 tol-1e-13 solution.  Every fifth case (and three
+fixed fractions 1e-5, 1e-3, 1e-1) is also pinned to the oracle on the CPU:
+the FP64 iterations are within max(1, 2 %) of the oracle CG's on the
+independently assembled E^T A E, and the FP64 tol-1e-13 solution is within
+1e-9 of the oracle's."""
 
 from __future__ import annotations
 
@@ -18,7 +22,24 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-EPS = [1e-5, 1e-3, 1e-1]
+N_ELEM, DEGREE = 16, 4
+FIXED = [1e-5, 1e-3, 1e-1]
+# iteration factor of the reduced-precision forms over plain FP64 at tol 1e-9
+# (measured on this set: FP32 within +25 %, two-plane BF16 within +55 %)
+ITER_FACTOR = {"fp32-ir": 1.35, "bf16-ir": 1.7}
+
+
+def _cases():
+    from cutcell_b200.workloads import sliver_stress_cases
+
+    cases = [(f"cut{k}", nrm, eps, k % 5 == 0) for k, (nrm, eps) in enumerate(sliver_stress_cases(25))]
+    rng = np.random.default_rng(12345)
+    for j, eps in enumerate(FIXED):
+        cases.append((f"fixed{j}", np.abs(rng.standard_normal(3)) + 1e-3, eps, True))
+    return cases
+
+
+CASES = _cases()
 
 
 @pytest.fixture(scope="module")
@@ -30,48 +51,51 @@ def torch_cuda():
     return torch
 
 
-def _case(k, eps):
+def _problem(nrm, eps):
     from cutcell_b200.aggregation import build_extension
     from cutcell_b200.problem import build_problem
-    from cutcell_b200.workloads import sliver_plane
-    from oracle.aggregation import restrict_spd
-    from oracle.assembly import assemble_full
+    from cutcell_b200.workloads import sliver_plane, stress_rhs
 
-    rng = np.random.default_rng(12345 + k)
-    phi = sliver_plane(16, rng.standard_normal(3), eps)
-    prob = build_problem(phi, 16, 4)
-    ext = build_extension(prob.gamma, prob.basis, 4)
-    A = restrict_spd(assemble_full(prob), ext.E).tocsr()
-    b = np.random.default_rng(12345).standard_normal(ext.n_red)
-    return prob, ext, A, b
+    phi = sliver_plane(N_ELEM, nrm, eps)
+    prob = build_problem(phi, N_ELEM, DEGREE)
+    ext = build_extension(prob.gamma, prob.basis, DEGREE)
+    b = stress_rhs(ext.n_red, N_ELEM, DEGREE)
+    return prob, ext, b
 
 
-@pytest.mark.parametrize("k,eps", list(enumerate(EPS)))
-def test_sliver_stress_mixed_precision(torch_cuda, k, eps):
+@pytest.mark.parametrize("name,nrm,eps,pinned", CASES, ids=[c[0] for c in CASES])
+def test_sliver_stress_mixed_precision(torch_cuda, name, nrm, eps, pinned):
     from cutcell_b200 import solve_spd
     from cutcell_b200.operator import CutCellOperator
-    from oracle.pcg import cg_loop
 
-    prob, ext, A, b = _case(k, eps)
+    prob, ext, b = _problem(nrm, eps)
     assert abs(prob.min_cut_fraction / eps - 1.0) < 1e-6
-    x_ref, rep_ref = cg_loop(A, b, tol=1e-13, maxiter=50000)
-    _, rep_o = cg_loop(A, b, tol=1e-9, maxiter=50000)
     op = CutCellOperator(prob, ext)
     try:
         x, rep = solve_spd(op, b, tol=1e-9, maxiter=50000)
         assert rep.success, rep
-        assert abs(rep.iterations - rep_o["iterations"]) <= max(1, 0.02 * rep_o["iterations"])
         x64, rep64 = solve_spd(op, b, tol=1e-13, maxiter=50000)
         assert rep64.success, rep64
-        assert np.linalg.norm(x64 - x_ref) / np.linalg.norm(x_ref) < 1e-9
-        x32, rep32 = solve_spd(op, b, tol=1e-13, maxiter=50000, precision="fp32-ir")
-        assert rep32.success, rep32
-        assert np.linalg.norm(x32 - x_ref) / np.linalg.norm(x_ref) < 1e-7
-        x16, rep16 = solve_spd(op, b, tol=1e-9, maxiter=50000, precision="bf16-ir")
-        if rep16.success:
-            assert np.linalg.norm(x16 - x_ref) / np.linalg.norm(x_ref) < 1e-7
-        else:
-            assert rep16.message in ("CG breakdown: non-positive curvature", "maximum iterations reached")
-            assert np.all(np.isfinite(x16))
+        its = {"fp64": rep.iterations}
+        for prec in ("fp32-ir", "bf16-ir"):
+            _, r9 = solve_spd(op, b, tol=1e-9, maxiter=50000, precision=prec)
+            assert r9.success, (prec, r9)
+            its[prec] = r9.iterations
+            assert r9.iterations <= ITER_FACTOR[prec] * rep.iterations, (prec, r9.iterations, rep.iterations)
+            x11, r11 = solve_spd(op, b, tol=1e-11, maxiter=50000, precision=prec)
+            assert r11.success, (prec, r11)
+            err = np.linalg.norm(x11 - x64) / np.linalg.norm(x64)
+            assert err < 1e-7, (prec, err)
+        print(f"{name} eps={eps:.2e} iterations {its}")
+        if pinned:
+            from oracle.aggregation import restrict_spd
+            from oracle.assembly import assemble_full
+            from oracle.pcg import cg_loop
+
+            A = restrict_spd(assemble_full(prob), ext.E).tocsr()
+            _, rep_o = cg_loop(A, b, tol=1e-9, maxiter=50000)
+            assert abs(rep.iterations - rep_o["iterations"]) <= max(1, 0.02 * rep_o["iterations"])
+            x_ref, _ = cg_loop(A, b, tol=1e-13, maxiter=50000)
+            assert np.linalg.norm(x64 - x_ref) / np.linalg.norm(x_ref) < 1e-9
     finally:
         op.close()
