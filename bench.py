@@ -49,13 +49,17 @@ def parse():
     ap.add_argument("--p", type=int, default=3)
     ap.add_argument("--radius", type=float, default=0.31)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--variants", default="fp64,fp32-ir,bf16-ir,learned")
+    ap.add_argument("--variants", default="fp64,fp32-ir,bf16-ir,block,learned")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batch / hill-step / cut-box summaries of the default run")
     ap.add_argument("--train-geometries", type=int, default=3)
     ap.add_argument("--train-pairs", type=int, default=20000)
     ap.add_argument("--workload", default="sphere", choices=["sphere", "hill", "hill-step", "batch", "apply"])
     ap.add_argument("--batch-count", type=int, default=72)
     ap.add_argument("--hill-nr", type=int, default=2345)
     ap.add_argument("--hill-nz", type=int, default=32)
+    ap.add_argument("--hill-nex", type=int, default=64)
+    ap.add_argument("--hill-ney", type=int, default=32)
+    ap.add_argument("--hill-build", default="real", choices=["real", "synthetic"])
     return ap.parse_args()
 
 
@@ -223,9 +227,10 @@ def run_batch_reference(args, rank, world):
     return 0
 
 
-def run_batch(args, rank, world, local):
+def run_batch(args, rank, world, local, emit=True):
     """72 uneven systems in one persistent, graph-captured launch (per rank:
-    its longest-processing-time share when several GPUs are used)."""
+    its longest-processing-time share when several GPUs are used).  With
+    emit=False the JSON line is returned instead of printed."""
     import torch
 
     from cutcell_b200.batch import BatchSolver, partition_lpt
@@ -233,7 +238,7 @@ def run_batch(args, rank, world, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    if world > 1:
+    if world > 1 and emit:
         import datetime
 
         import torch.distributed as dist
@@ -354,6 +359,9 @@ def run_batch(args, rank, world, local):
         cs = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": k / cs, "unit": "solves/s", "cores": 1, "kind": "port",
                                 "sample": f"first {k} of the {len(systems)} systems, sequential SciPy CG", **host_cpu()}
+    if not emit:
+        bs.close()
+        return line
     if rank == 0:
         print(json.dumps(line), flush=True)
     bs.close()
@@ -376,9 +384,15 @@ def run_reference(args, rank, world):
     from oracle.aggregation import restrict_spd
     from oracle.pcg import solve_cpu_cg
 
-    prob, ext = sphere_poisson(args.n, args.p, args.radius)
+    # the system is built by the NumPy host setup (no native library of this
+    # package is loaded in this arm) and assembled by the oracle
+    from oracle.assembly import assemble_full
+
+    t_setup = time.perf_counter()
+    prob, ext = sphere_poisson(args.n, args.p, args.radius, native=False)
     b = np.asarray(ext.E.T @ prob.load)
-    A = restrict_spd(prob.assemble_full_csr(), ext.E)
+    A = restrict_spd(assemble_full(prob), ext.E)
+    t_setup = time.perf_counter() - t_setup
     for _ in range(args.warmup):
         solve_cpu_cg(A, b, tol=TOL, maxiter=20000)
     ts = []
@@ -403,7 +417,8 @@ def run_reference(args, rank, world):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded geometry, manufactured forcing)",
-        "config": {"workload": f"sphere-cut Poisson p={args.p} n={args.n} r={args.radius}", "n_red": ext.n_red, "nnz": int(A.nnz), "iterations": it},
+        "config": {"workload": f"sphere-cut Poisson p={args.p} n={args.n} r={args.radius}", "n_red": ext.n_red, "nnz": int(A.nnz), "iterations": it,
+                   "setup": "NumPy cut quadrature + oracle assembly (no native code of this package)", "setup_s": t_setup},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": "full solve per step (SciPy CSR SpMV is single-threaded)", **host_cpu()},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -473,40 +488,60 @@ def run_hill(args, rank, world, local):
     return 0
 
 
-def run_hill_step(args, rank, world, local):
+def run_hill_step(args, rank, world, local, emit=True):
     """One hill_fastdiag_step (SSP-RK3 skew advection + fast-diagonalisation
-    solve) at the channel configuration's sizes: nr = 2345 reduced 2D modes
-    (64 x 32 elements, p = 3), nz = 32, 64 x 32 cells of 14 x 14 Gauss points
-    (n2q = 401,408) with 16 modes per sample row, 9 z points per element.
-    Sample machinery and operators are seeded synthetic stand-ins of those
-    shapes (the reference builds them in hours on the CPU)."""
+    solve) on the periodic-hill channel: 64 x 32 x-y elements, nz = 32,
+    p = 3, physical metric (Lx = 9, Ly = 3.036, Lz = 4.5), nu = 1/5600,
+    dt = 0.02, from the parabolic initial condition with a 1 % perturbation.
+    The channel is built by the anisotropic restatement of Hill3D::build
+    (cutcell_b200.hillsetup) and its per-mode operators on the device through
+    the shared eigenbasis.  ``--hill-build synthetic`` times seeded stand-ins
+    of the same shapes instead."""
     import torch
 
     from cutcell_b200.hill import FastDiagHill, HillAdvection, synthetic_machinery
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    nr, nz = args.hill_nr, args.hill_nz
+    nz = args.hill_nz
     t0 = time.perf_counter()
-    m = synthetic_machinery(nr=nr, nz=nz, cells=(64, 32), pts_per_cell=196, modes_per_row=16)
-    adv = HillAdvection(m["phi"], m["dpx"], m["dpy"], m["w2"], m["Vz"], m["dVz"], m["wz"], m["M2inv"], m["Mzinv"],
-                        device=dev)
-    g = torch.Generator(device=dev).manual_seed(20260629)
-    rnd = lambda *shape: torch.randn(*shape, generator=g, device=dev, dtype=torch.float64) / np.sqrt(shape[-1])
-    M2, Qx2, Qy2 = rnd(nr, nr), rnd(nr, nr), rnd(nr, nr)
-    Mz_row = np.zeros(nz); Mz_row[0], Mz_row[1], Mz_row[-1] = 0.6, 0.2, 0.2
-    Sz_row = np.zeros(nz); Sz_row[0], Sz_row[1], Sz_row[-1] = 2.0, -1.0, -1.0
-    Kz_row = np.zeros(nz); Kz_row[1], Kz_row[-1] = 0.5, -0.5
-    Ainv, Sinv = rnd(nz, nr, nr), rnd(nz, nr, nr)
-    fd = FastDiagHill(device=dev).build(M2, Qx2, Qy2, None, Mz_row, Sz_row, Kz_row, 0.01, inverses=(Ainv, Sinv))
-    setup_s = time.perf_counter() - t0
-    u0 = [0.1 * rnd(nr, nz) for _ in range(3)]
+    dt, nu = 0.02, 1.0 / 5600.0
+    hs = None
+    if args.hill_build == "real":
+        from cutcell_b200.hillsetup import build_hill, parabolic_ic
+
+        hs = build_hill(args.hill_nex, args.hill_ney, 3, nz, 4.5, physical=True)
+        host_build_s = time.perf_counter() - t0
+        m = hs.machinery()
+        nr = hs.nr
+        adv = HillAdvection(m["phi"], m["dpx"], m["dpy"], m["w2"], m["Vz"], m["dVz"], m["wz"], m["M2inv"],
+                            m["Mzinv"], device=dev)
+        fd = FastDiagHill(device=dev).build(hs.M2, hs.Qx2, hs.Qy2, hs.KN2, hs.Mz[0], hs.Sz[0], hs.Kz[0], dt * nu,
+                                            on_device=True)
+        u0 = [torch.as_tensor(np.ascontiguousarray(c)).to(dev) for c in parabolic_ic(hs)]
+        setup_s = time.perf_counter() - t0
+    else:
+        nr = args.hill_nr
+        m = synthetic_machinery(nr=nr, nz=nz, cells=(64, 32), pts_per_cell=196, modes_per_row=16)
+        adv = HillAdvection(m["phi"], m["dpx"], m["dpy"], m["w2"], m["Vz"], m["dVz"], m["wz"], m["M2inv"],
+                            m["Mzinv"], device=dev)
+        g = torch.Generator(device=dev).manual_seed(20260629)
+        rnd = lambda *shape: torch.randn(*shape, generator=g, device=dev, dtype=torch.float64) / np.sqrt(shape[-1])
+        M2, Qx2, Qy2 = rnd(nr, nr), rnd(nr, nr), rnd(nr, nr)
+        Mz_row = np.zeros(nz); Mz_row[0], Mz_row[1], Mz_row[-1] = 0.6, 0.2, 0.2
+        Sz_row = np.zeros(nz); Sz_row[0], Sz_row[1], Sz_row[-1] = 2.0, -1.0, -1.0
+        Kz_row = np.zeros(nz); Kz_row[1], Kz_row[-1] = 0.5, -0.5
+        Ainv, Sinv = rnd(nz, nr, nr), rnd(nz, nr, nr)
+        fd = FastDiagHill(device=dev).build(M2, Qx2, Qy2, None, Mz_row, Sz_row, Kz_row, 0.01, inverses=(Ainv, Sinv))
+        u0 = [0.1 * rnd(nr, nz) for _ in range(3)]
+        host_build_s = 0.0
+        setup_s = time.perf_counter() - t0
     u = [t.clone() for t in u0]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     for _ in range(args.warmup):
         for a, b in zip(u, u0):
             a.copy_(b)
-        adv.step(fd, u, 0.02, 0.7)
+        adv.step(fd, u, dt, 0.0)
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
@@ -518,7 +553,7 @@ def run_hill_step(args, rank, world, local):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        adv.step(fd, u, 0.02, 0.7)
+        adv.step(fd, u, dt, 0.0)
         e1.record()
         torch.cuda.synchronize()
         ms.append(e0.elapsed_time(e1))
@@ -533,18 +568,32 @@ def run_hill_step(args, rank, world, local):
     t = float(np.mean(ms))
     ta = float(np.mean(ms_adv))
     n2q, nzq = m["phi"].shape[0], m["Vz"].shape[0]
-    L = m["phi"].nnz // n2q
+    L = round(m["phi"].nnz / n2q)
     # FP64 flops of one skew_conv of three components (fused kernel), per 2D point:
     # 2D sample 9 L nz FMA, z band 3 x (qpe x nz) x (48 + 12 FMA + ~10), 2D load 9 L nz FMA
     flop_adv = 2.0 * n2q * (18 * L * nz + 3 * nzq * 70) + 2.0 * nr * nr * 3 * nz
+    div = None
+    if hs is not None:
+        from cutcell_b200.hillsetup import weak_div
+
+        uh = [c.cpu().numpy() for c in u]
+        d0 = float(np.abs(weak_div(hs, *[c.cpu().numpy() for c in u0])).max())
+        d1 = float(np.abs(weak_div(hs, *uh)).max())
+        div = {"max_abs_initial": d0, "max_abs_after_step": d1, "ratio": d1 / d0,
+               "max_abs_u": float(max(np.abs(c).max() for c in uh)),
+               "note": "weak divergence hill_weak_div (hill3d.h:330-334) of the stepped velocity"}
     line = {
         "metric": "ms per hill fast step (SSP-RK3 skew advection + fast-diagonalisation solve)",
         "value": t, "unit": "ms/step", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic sample machinery and operators of the configuration's sizes (seeded)",
-        "config": {"workload": f"hill fast step nr={nr} nz={nz} n2q={n2q} nzq={nzq} row_nnz={L}",
-                   "l2": "flushed between timed steps", "setup_s": setup_s, "advect_ms": ta,
-                   "advect_gflops": flop_adv / (ta * 1e-3) / 1e9},
+        "data": ("periodic-hill channel built by the anisotropic Hill3D::build restatement, parabolic IC + 1 % seeded "
+                 "perturbation" if hs is not None else "synthetic sample machinery and operators of the configuration's sizes (seeded)"),
+        "config": {"workload": (f"hill channel {args.hill_nex}x{args.hill_ney} elements nz={nz} p=3 physical metric "
+                                f"(nr={nr} n2q={n2q} nzq={nzq} row_nnz={L})" if hs is not None else
+                                f"hill fast step nr={nr} nz={nz} n2q={n2q} nzq={nzq} row_nnz={L}"),
+                   "l2": "flushed between timed steps", "setup_s": setup_s, "host_build_s": host_build_s,
+                   "fastdiag_build": getattr(fd, "build_timings", None), "advect_ms": ta,
+                   "advect_gflops": flop_adv / (ta * 1e-3) / 1e9, "divergence": div, "dt": dt, "nu": nu},
         "clocks": clocks, "gpu_launches": (3 * 4 + 3 + 15) * args.steps,
         # the advection kernel is FP64-FMA bound (no tensor-core FP64 kind on this path);
         # peak: B200 FP64 nominal, not measured on this pool
@@ -553,6 +602,10 @@ def run_hill_step(args, rank, world, local):
                      "frac": flop_adv / (ta * 1e-3) / 1e12 / 37.0, "peak_kind": "nominal",
                      "traffic": NCU_TRAFFIC.get(("hill-step",))},
     }
+    if not emit:
+        adv.close()
+        fd.close()
+        return line
     if rank == 0:
         print(json.dumps(line), flush=True)
     adv.close()
@@ -666,24 +719,33 @@ def main():
     wanted = args.variants.split(",")
     if "learned" in wanted:
         # training on random sphere radii in [0.2, 0.4] with the project's kernels
-        from cutcell_b200.learned import PatchMLP, attach, generate_pairs, train
+        from cutcell_b200.learned import PatchMLP, attach, attach_blocks, fit_linear, generate_pairs, train
 
         t0 = time.perf_counter()
         rng = np.random.default_rng(20260629)
         radii = [float(r) for r in rng.uniform(0.2, 0.4, args.train_geometries)]
         train_ops = [CutCellOperator(*sphere_poisson(args.n, args.p, r), device=dev) for r in radii]
         X, T = generate_pairs(train_ops, args.train_pairs, seed=11)
-        net = PatchMLP(seed=2)
-        hist = train(net, X, T, epochs=40, batch=512, lr=1e-3)
+        # least-squares start of the identity-activation network, then Adam
+        # fine-tuning with the project's training kernels
+        net = PatchMLP(fit_linear(X, T), activation="identity")
+        hist = train(net, X, T, epochs=4, batch=512, lr=1e-5)
         attach(op, net)
         for o in train_ops:
             o.close()
         learned_info = {"radii": radii, "pairs": int(X.shape[0]), "loss_first": hist[0], "loss_last": hist[-1],
-                        "train_s": time.perf_counter() - t0}
+                        "target_mean_square": float((T.double() ** 2).mean()), "train_s": time.perf_counter() - t0,
+                        "canonical_patches": int(op._patch_solves.canonical.sum()) if hasattr(op, "_patch_solves") else None}
+    t_blocks = None
     for prec in wanted:
         solve_kw = {"precision": prec}
-        if prec == "learned":
-            solve_kw = {"precision": "fp64", "preconditioner": "jacobi+learned"}
+        if prec in ("learned", "block"):
+            from cutcell_b200.learned import attach_blocks
+
+            t0 = time.perf_counter()
+            attach_blocks(op, "noncanonical" if prec == "learned" else "all")
+            t_blocks = t_blocks or time.perf_counter() - t0
+            solve_kw = {"precision": "fp64", "preconditioner": "jacobi+learned" if prec == "learned" else "block"}
         elif prec != "fp64":
             op.set_refinement(0.1)
         for _ in range(args.warmup):
@@ -736,7 +798,11 @@ def main():
     # end-to-end through the public API, host buffers (pinned), H2D + D2H inside
     b_pin = torch.from_numpy(b_host).pin_memory()
     e2e_prec = best_key
-    e2e_kw = {"precision": e2e_prec} if e2e_prec != "learned" else {"preconditioner": "jacobi+learned"}
+    e2e_kw = {"precision": e2e_prec}
+    if e2e_prec == "learned":
+        e2e_kw = {"preconditioner": "jacobi+learned"}
+    elif e2e_prec == "block":
+        e2e_kw = {"preconditioner": "block"}
     for _ in range(2):
         solve_spd(op, b_pin.numpy(), tol=TOL, maxiter=20000, **e2e_kw)
     barrier()
@@ -799,6 +865,10 @@ def main():
             **host_cpu(),
         }
         line["config"]["cpu_rel_err_vs_gpu_fp64"] = float(np.linalg.norm(xc - ref_x) / np.linalg.norm(xc))
+    if t_blocks is not None:
+        line["config"]["patch_blocks_setup_s"] = t_blocks
+    if world == 1 and not args.no_extras:
+        line["extras"] = extras_summary(args, rank, world, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     op.close()
@@ -807,6 +877,81 @@ def main():
 
         dist.destroy_process_group()
     return 0
+
+
+def run_cutbox(args, dev, steps: int, n: int = 64, p: int = 3):
+    """The tensor cut-box Poisson system of solve_poisson_3d (cuts at
+    fractions 0.6 on all three axes) solved matrix-free with the Kronecker
+    operator: Jacobi-PCG to 1e-9 (device time) and one apply of the Poisson
+    form, L2 flushed between launches."""
+    import torch
+
+    from cutcell_b200 import tensorbox as tb
+
+    t0 = time.perf_counter()
+    box = tb.cut_box(n, p, (0.6, 0.6, 0.6))
+    rhs = tb.poisson_rhs(box)
+    op = tb.KronOperator(box, device=dev)
+    setup_s = time.perf_counter() - t0
+    b = torch.as_tensor(rhs).to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    x, rep = op.solve_device(b, tol=TOL, maxiter=20000)
+    ms, ams = [], []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        x, rep = op.solve_device(b, tol=TOL, maxiter=20000)
+        ms.append(float(rep.elapsed_ms))
+        flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        op.apply(b, "A")
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ams.append(e0.elapsed_time(e1))
+    N = box.n_red
+    # algorithmic bytes of one apply: p read, y written, and the four pass
+    # buffers each written once and read once (x pass writes U1 U2, y pass
+    # reads them and writes V1 V2, z pass reads V1 V2)
+    bytes_apply = 8.0 * N * (1 + 1 + 2 * 4)
+    hbm, hbm_kind = peaks()
+    am = float(np.median(ams))
+    op.close()
+    return {
+        "workload": f"tensor cut box p={p} n={n} fractions (0.6,0.6,0.6), weak-penalty Poisson, Kronecker operator",
+        "n_red": N, "iterations": int(rep.iterations), "converged": bool(rep.status == 0),
+        "s_per_solve": float(np.mean(ms)) / 1e3, "apply_us": am * 1e3, "setup_s": setup_s,
+        "roofline_apply": {"bound": "hbm", "achieved": bytes_apply / (am * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                           "frac": bytes_apply / (am * 1e-3) / 1e9 / hbm, "peak_kind": hbm_kind,
+                           "algorithmic_bytes": bytes_apply},
+    }
+
+
+def extras_summary(args, rank, world, local):
+    """Driver-measured summaries of the other hot-path workloads, run in the
+    default invocation at few steps: the 72-system batch, the hill fast step
+    and the tensor cut-box solve (each also has its own --workload line)."""
+    import copy
+
+    import torch
+
+    dev = torch.device("cuda", local)
+    sub = copy.copy(args)
+    sub.steps, sub.warmup = min(args.steps, 5), min(args.warmup, 3)
+    out = {}
+    bl = run_batch(sub, rank, world, local, emit=False)
+    out["batch"] = {k: bl[k] for k in ("metric", "value", "unit", "ms_per_step", "e2e")}
+    out["batch"].update({"sequential_solves_per_s": bl["sequential"]["solves_per_s"],
+                         "all_converged": bl["config"]["all_converged"], "autotuned": bl["config"]["autotuned"],
+                         "roofline_frac": bl["roofline"]["frac"], "workload": bl["config"]["workload"]})
+    hl = run_hill_step(sub, rank, world, local, emit=False)
+    out["hill_step"] = {k: hl[k] for k in ("metric", "value", "unit", "data")}
+    out["hill_step"].update({"workload": hl["config"]["workload"], "advect_ms": hl["config"]["advect_ms"],
+                             "roofline": hl["roofline"], "divergence": hl["config"]["divergence"],
+                             "setup_s": hl["config"]["setup_s"], "fastdiag_build": hl["config"]["fastdiag_build"]})
+    out["cut_box"] = run_cutbox(args, dev, sub.steps)
+    return out
 
 
 if __name__ == "__main__":

@@ -13,6 +13,7 @@
 #include "learned.cuh"
 #include "fastdiag.cuh"
 #include "kron.cuh"
+#include "dgemm.cuh"
 
 namespace {
 
@@ -186,7 +187,8 @@ struct cutcell_ctx {
     int max_blocks = 0;
     // learned preconditioner
     cutcell_mlp* mlp = nullptr;
-    PatchMap pmap = {0, nullptr, nullptr, nullptr};
+    PatchMap pmap = {0, nullptr, nullptr, nullptr, nullptr};
+    int* pslot_all = nullptr;  // identity patch -> block map of cutcell_pcg_set_block_inverses
     double* zl = nullptr;
     double* rold = nullptr;
     // reduced-precision forms: residual-replacement factor and cap
@@ -277,7 +279,8 @@ static int run_ru(cutcell_ctx* c, const OpHi& hi, const OpLo& lo, size_t smem, S
 }
 
 template <class Op>
-static int run_fcg(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, cudaStream_t s, int* blocks) {
+static int run_fcg(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, cudaStream_t s, int* blocks,
+                   int mode) {
     auto kern = fcg_kernel<Op>;
     const size_t op_al = (op_smem + 15) & ~(size_t)15;
     const size_t smem = op_al + MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 3 * 64) * sizeof(float);
@@ -286,11 +289,12 @@ static int run_fcg(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, c
     a.gs = make_gs(c, *blocks);
     a.B = make_bufs(c);
     LearnedArgs L;
-    L.W = c->mlp->weights();
+    memset(&L, 0, sizeof(L));
+    if (mode == 1) L.W = c->mlp->weights();
     L.pm = c->pmap;
     L.z = c->zl;
     L.rold = c->rold;
-    L.use_mlp = c->pmap.binv ? 2 : 1;
+    L.use_mlp = mode;
     return launch_coop(kern, *blocks, smem, s, op, a, L, op_al);
 }
 
@@ -318,7 +322,8 @@ static int tiles_run(cutcell_ctx* c, int mode, int precision, SolveArgs* a, cons
     TileOp<float, P1> o32{c->td, c->cut32};
     TileOp<bf16x2_t, P1> o16{c->td, c->cut16};
     const size_t sm = TileOp<double, P1>::smem_bytes();
-    if (mode == 2) return run_fcg(c, o64, sm, *a, s, blocks);
+    if (mode == 2) return run_fcg(c, o64, sm, *a, s, blocks, 1);
+    if (mode == 3) return run_fcg(c, o64, sm, *a, s, blocks, 2);
     if (mode == 1) {
         if (precision == CUTCELL_FP64) return run_apply(c, o64, sm, x, y, s);
         if (precision == CUTCELL_FP32_IR) return run_apply(c, o32, sm, x, y, s);
@@ -796,6 +801,19 @@ int cutcell_apply_form(cutcell_ctx* c, const double* x, double* y, int32_t which
     return cutcell_apply(c, x, y, CUTCELL_FP64, stream);
 }
 
+int cutcell_dgemm_nt(int32_t M, int32_t N, int32_t K, const double* A, int64_t lda, int64_t strideA, const double* B,
+                     int64_t ldb, int64_t strideB, const double* s, int64_t strideS, double beta, double* C, int64_t ldc,
+                     int64_t strideC, int32_t batch, void* stream) {
+    if (M < 0 || N < 0 || K < 0 || batch < 0 || !A || !B || !C || lda < K || ldb < K || ldc < N) return CUTCELL_E_ARG;
+    if (M == 0 || N == 0 || batch == 0) return CUTCELL_OK;
+    if (batch > 65535 || ceil_div(M, DG_BM) > 65535) return CUTCELL_E_SHAPE;
+    DgemmArgs g{M, N, K, A, lda, strideA, B, ldb, strideB, s, strideS, beta, C, ldc, strideC};
+    dim3 grid(ceil_div(N, DG_BN), ceil_div(M, DG_BM), batch);
+    dgemm_nt_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(g);
+    CK(cudaGetLastError());
+    return CUTCELL_OK;
+}
+
 int cutcell_set_refinement(cutcell_ctx* c, double replace_factor, int32_t reserved, int32_t max_replacements) {
     if (!c || !(replace_factor > 0.0 && replace_factor < 1.0) || max_replacements < 1) return CUTCELL_E_ARG;
     (void)reserved;
@@ -808,9 +826,14 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
                       int32_t precond, CutcellReport* report, void* stream) {
     if (!c || !b || !x || maxiter < 0 || !(tol >= 0.0)) return CUTCELL_E_ARG;
     if (precision < CUTCELL_FP64 || precision > CUTCELL_BF16_IR) return CUTCELL_E_ARG;
-    if (precond < CUTCELL_PRECOND_NONE || precond > CUTCELL_PRECOND_JACOBI_LEARNED) return CUTCELL_E_ARG;
+    if (precond < CUTCELL_PRECOND_NONE || precond > CUTCELL_PRECOND_BLOCK) return CUTCELL_E_ARG;
     if (precond == CUTCELL_PRECOND_JACOBI_LEARNED && (!c->mlp || precision != CUTCELL_FP64 || c->kind != KIND_TILES))
         return CUTCELL_E_ARG;
+    if (precond == CUTCELL_PRECOND_BLOCK &&
+        (!c->pmap.binv || !c->pmap.slot || !c->zl || precision != CUTCELL_FP64 || c->kind != KIND_TILES)) {
+        g_last_error = "CUTCELL_PRECOND_BLOCK needs patch blocks (cutcell_pcg_set_patch_blocks), FP64, a tile context";
+        return CUTCELL_E_ARG;
+    }
     if (c->kind == KIND_KRON && precision != CUTCELL_FP64) {
         g_last_error = "the Kronecker cut-box operator is solved in FP64";
         return CUTCELL_E_ARG;
@@ -845,6 +868,8 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
             st = run_ru(c, c->csr64, c->csr16, 0, a, s, &blocks);
     } else if (precond == CUTCELL_PRECOND_JACOBI_LEARNED) {
         st = tiles_dispatch(c, 2, precision, &a, nullptr, nullptr, s, &blocks);
+    } else if (precond == CUTCELL_PRECOND_BLOCK) {
+        st = tiles_dispatch(c, 3, precision, &a, nullptr, nullptr, s, &blocks);
     } else {
         st = tiles_dispatch(c, 0, precision, &a, nullptr, nullptr, s, &blocks);
     }
@@ -908,7 +933,7 @@ int cutcell_ext_scatter(cutcell_ctx* c, const double* y_full, double* y_red, voi
 int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);  // cudaFree below waits for the work that may still use the buffers
-    void* bufs[] = {c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->pslot_all, c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
                     c->p,     c->p2,    c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -1002,7 +1027,7 @@ int cutcell_patch_features(cutcell_ctx* c, const int32_t* patch_red, const float
                            const double* r, float* X, float* S, void* stream) {
     if (!c || !patch_red || !patch_gamma || !r || !X || !S || n_patch < 0) return CUTCELL_E_ARG;
     if (n_patch == 0) return CUTCELL_OK;
-    PatchMap pm{n_patch, patch_red, patch_gamma, nullptr};
+    PatchMap pm{n_patch, patch_red, patch_gamma, nullptr, nullptr};
     patch_features_kernel<<<ceil_div(n_patch, CUTCELL_WARPS), CUTCELL_BLOCK, 0, (cudaStream_t)stream>>>(pm, r, c->dinv,
                                                                                                       X, S);
     CK(cudaGetLastError());
@@ -1013,15 +1038,54 @@ int cutcell_patch_targets(cutcell_ctx* c, const int32_t* patch_red, int32_t n_pa
                           const double* r, const float* S, float* T, void* stream) {
     if (!c || !patch_red || !e || !r || !S || !T || n_patch < 0) return CUTCELL_E_ARG;
     if (n_patch == 0) return CUTCELL_OK;
-    PatchMap pm{n_patch, patch_red, nullptr, nullptr};
+    PatchMap pm{n_patch, patch_red, nullptr, nullptr, nullptr};
     patch_targets_kernel<<<ceil_div((long)n_patch * 64, 256), 256, 0, (cudaStream_t)stream>>>(pm, e, r, c->dinv, S, T);
     CK(cudaGetLastError());
     return CUTCELL_OK;
 }
 
 int cutcell_pcg_set_block_inverses(cutcell_ctx* c, const double* binv) {
-    if (!c || c->kind != KIND_TILES || !c->mlp) return CUTCELL_E_ARG;
+    if (!c || c->kind != KIND_TILES || c->pmap.n_patch <= 0) return CUTCELL_E_ARG;
+    if (!binv) {
+        c->pmap.binv = nullptr;
+        c->pmap.slot = nullptr;
+        return CUTCELL_OK;
+    }
+    if (!c->pslot_all) {
+        std::vector<int> id(c->pmap.n_patch);
+        for (int k = 0; k < c->pmap.n_patch; ++k) id[k] = k;
+        CK(cudaMalloc(&c->pslot_all, id.size() * sizeof(int)));
+        CK(cudaMemcpy(c->pslot_all, id.data(), id.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     c->pmap.binv = binv;
+    c->pmap.slot = c->pslot_all;
+    return CUTCELL_OK;
+}
+
+int cutcell_pcg_set_patch_blocks(cutcell_ctx* c, const int32_t* patch_red, int32_t n_patch, const int32_t* slot,
+                                 const double* binv) {
+    if (!c || c->kind != KIND_TILES) return CUTCELL_E_ARG;
+    if (!binv) {
+        c->pmap.binv = nullptr;
+        c->pmap.slot = nullptr;
+        return CUTCELL_OK;
+    }
+    if (!patch_red || !slot || n_patch <= 0) return CUTCELL_E_ARG;
+    if (c->mlp && (c->pmap.red != patch_red || c->pmap.n_patch != n_patch)) {
+        g_last_error = "patch blocks must use the layout of the attached network";
+        return CUTCELL_E_ARG;
+    }
+    if (!c->mlp) {
+        c->pmap.red = patch_red;
+        c->pmap.n_patch = n_patch;
+        c->pmap.gamma = nullptr;
+    }
+    c->pmap.binv = binv;
+    c->pmap.slot = slot;
+    if (!c->zl) {
+        CK(cudaMalloc(&c->zl, (size_t)c->n * sizeof(double)));
+        CK(cudaMalloc(&c->rold, (size_t)c->n * sizeof(double)));
+    }
     return CUTCELL_OK;
 }
 
@@ -1030,7 +1094,9 @@ int cutcell_pcg_set_learned(cutcell_ctx* c, cutcell_mlp* m, const int32_t* patch
     if (!c || c->kind != KIND_TILES) return CUTCELL_E_ARG;
     if (m && (!patch_red || !patch_gamma || n_patch <= 0)) return CUTCELL_E_ARG;
     c->mlp = m;
-    c->pmap = PatchMap{n_patch, patch_red, patch_gamma, nullptr};
+    // patch blocks set for the same layout stay attached
+    const bool keep = c->pmap.binv && c->pmap.red == patch_red && c->pmap.n_patch == n_patch;
+    c->pmap = PatchMap{n_patch, patch_red, patch_gamma, keep ? c->pmap.binv : nullptr, keep ? c->pmap.slot : nullptr};
     if (m && !c->zl) {
         CK(cudaMalloc(&c->zl, (size_t)c->n * sizeof(double)));
         CK(cudaMalloc(&c->rold, (size_t)c->n * sizeof(double)));

@@ -276,7 +276,8 @@ struct PatchMap {
     int n_patch;
     const int* red;      // [n_patch][64] reduced index or -1
     const float* gamma;  // [n_patch][64]
-    const double* binv;  // optional [n_patch][64][64] exact patch inverses (block Jacobi)
+    const double* binv;  // optional exact patch inverses [n_blocks][64][64], symmetric
+    const int* slot;     // optional [n_patch]: block of the patch in binv, or -1 (network / Jacobi)
 };
 
 __device__ __forceinline__ float patch_features_warp(const PatchMap& pm, int k, const double* r, const double* dinv,
@@ -323,16 +324,42 @@ __global__ void patch_targets_kernel(PatchMap pm, const double* e, const double*
 }
 
 // ---------------------------------------------------------------------------
-// Flexible PCG with z = D^{-1} r + s * mlp(x) (Polak-Ribiere beta).
-// Safeguard: if r.z_mlp <= 0.1 * r.D^{-1}r the iteration uses Jacobi.
+// Flexible PCG with the patch preconditioner z = M(r): exact patch blocks
+// where given, the network z = D^{-1} r + s * mlp(x) or Jacobi on the other
+// patches (Polak-Ribiere beta).
+// Safeguard: if r.z <= 0.1 * r.D^{-1}r the iteration uses Jacobi.
 // ---------------------------------------------------------------------------
+// Patch preconditioner modes (LearnedArgs::use_mlp):
+//   1: patches with an exact block use it, the others the network;
+//   2: patches with an exact block use it, the others Jacobi (block Jacobi,
+//      the method without the network).
 struct LearnedArgs {
     MlpWeights W;
     PatchMap pm;
-    double* z;      // [n] learned correction target
+    double* z;      // [n] preconditioned residual
     double* rold;   // [n]
     int use_mlp;
 };
+
+// z_P = B_P^-1 r_P by one warp; B_P is symmetric, so lane l accumulates rows
+// l and l + 32 from the columns, each column one coalesced 512-byte read.
+__device__ __forceinline__ void patch_block_solve(const LearnedArgs& L, const PcgBufs& B, int k, int slot) {
+    const int l = threadIdx.x & 31;
+    double rp0 = 0.0, rp1 = 0.0;
+    const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
+    if (j0 >= 0) rp0 = __ldcg(B.r + j0);
+    if (j1 >= 0) rp1 = __ldcg(B.r + j1);
+    double z0 = 0.0, z1 = 0.0;
+    const double* Bk = L.pm.binv + (size_t)slot * 4096;
+#pragma unroll 8
+    for (int q = 0; q < 64; ++q) {
+        const double rq = __shfl_sync(0xffffffffu, q < 32 ? rp0 : rp1, q & 31);
+        z0 += __ldg(Bk + q * 64 + l) * rq;
+        z1 += __ldg(Bk + q * 64 + l + 32) * rq;
+    }
+    if (j0 >= 0) L.z[j0] = z0;
+    if (j1 >= 0) L.z[j1] = z1;
+}
 
 __device__ __forceinline__ void learned_precond_phase(const LearnedArgs& L, const PcgBufs& B, const MlpSmem& S,
                                                       float* scratch) {
@@ -342,28 +369,21 @@ __device__ __forceinline__ void learned_precond_phase(const LearnedArgs& L, cons
     float* h2 = h1 + 64;
     float* y = h2 + 64;
     const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
-    if (L.use_mlp == 2) {  // exact block Jacobi on the patches (reference ceiling)
-        for (int k = gw; k < L.pm.n_patch; k += nw) {
-            double rp0 = 0.0, rp1 = 0.0;
-            const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
-            if (j0 >= 0) rp0 = __ldcg(B.r + j0);
-            if (j1 >= 0) rp1 = __ldcg(B.r + j1);
-            double z0 = 0.0, z1 = 0.0;
-            const double* Bk = L.pm.binv + (size_t)k * 4096;
-            for (int q = 0; q < 64; ++q) {
-                const double rq = __shfl_sync(0xffffffffu, q < 32 ? rp0 : rp1, q & 31);
-                z0 += __ldg(Bk + l * 64 + q) * rq;
-                z1 += __ldg(Bk + (l + 32) * 64 + q) * rq;
-            }
-            if (j0 >= 0) L.z[j0] = z0;
-            if (j1 >= 0) L.z[j1] = z1;
-        }
-        return;
-    }
-    // odd part of the network in the residual: y = (f(u, g) - f(-u, g)) / 2,
-    // so the correction is linear under sign changes of r like the patch
-    // inverse it approximates
     for (int k = gw; k < L.pm.n_patch; k += nw) {
+        const int slot = (L.pm.binv && L.pm.slot) ? __ldg(L.pm.slot + k) : -1;
+        if (slot >= 0) {
+            patch_block_solve(L, B, k, slot);
+            continue;
+        }
+        const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
+        if (L.use_mlp != 1) {  // block Jacobi: Jacobi on patches without a block
+            if (j0 >= 0) L.z[j0] = B.dinv[j0] * __ldcg(B.r + j0);
+            if (j1 >= 0) L.z[j1] = B.dinv[j1] * __ldcg(B.r + j1);
+            continue;
+        }
+        // odd part of the network in the residual: y = (f(u, g) - f(-u, g)) / 2,
+        // so the correction is linear under sign changes of r like the patch
+        // inverse it approximates
         const float s = patch_features_warp(L.pm, k, B.r, B.dinv, xs);
         mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
         const float yp0 = y[l], yp1 = y[l + 32];
@@ -375,7 +395,6 @@ __device__ __forceinline__ void learned_precond_phase(const LearnedArgs& L, cons
         __syncwarp();
         mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
         const float ya = 0.5f * (yp0 - y[l]), yb = 0.5f * (yp1 - y[l + 32]);
-        const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
         if (j0 >= 0) L.z[j0] = B.dinv[j0] * __ldcg(B.r + j0) + (double)s * (double)ya;
         if (j1 >= 0) L.z[j1] = B.dinv[j1] * __ldcg(B.r + j1) + (double)s * (double)yb;
         __syncwarp();

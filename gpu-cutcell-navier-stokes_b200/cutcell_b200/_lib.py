@@ -31,6 +31,7 @@ PRECISIONS = {"fp64": FP64, "fp32-ir": FP32_IR, "bf16-ir": BF16_IR}
 PRECOND_NONE = 0
 PRECOND_JACOBI = 1
 PRECOND_JACOBI_LEARNED = 2
+PRECOND_BLOCK = 3
 MLP_NPARAM = 16576
 MLP_IN, MLP_H, MLP_OUT = 128, 64, 64
 
@@ -139,9 +140,12 @@ SIGNATURES = {
     "cutcell_patch_targets": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P, _P, _P]),
     "cutcell_pcg_set_learned": (C.c_int, [_P, _P, _P, _P, C.c_int32]),
     "cutcell_pcg_set_block_inverses": (C.c_int, [_P, _P]),
+    "cutcell_pcg_set_patch_blocks": (C.c_int, [_P, _P, C.c_int32, _P, _P]),
     "cutcell_fastdiag_create": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "cutcell_fastdiag_solve": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
     "cutcell_fastdiag_destroy": (C.c_int, [_P]),
+    "cutcell_dgemm_nt": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, C.c_int64, _P, C.c_int64, C.c_int64,
+                                   _P, C.c_int64, C.c_double, _P, C.c_int64, C.c_int64, C.c_int32, _P]),
     "cutcell_hill_create": (C.c_int, [C.POINTER(CutcellHillDesc), C.POINTER(_P)]),
     "cutcell_hill_skew_conv": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
     "cutcell_hill_step": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, C.c_double, _P]),

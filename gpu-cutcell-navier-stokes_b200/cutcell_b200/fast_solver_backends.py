@@ -27,7 +27,7 @@ import scipy.sparse as sp
 from . import _lib
 
 Backend = Literal["b200", "gpu", "auto"]
-Preconditioner = Literal["none", "jacobi", "jacobi+learned"]
+Preconditioner = Literal["none", "jacobi", "jacobi+learned", "block"]
 Precision = Literal["fp64", "fp32-ir", "bf16-ir"]
 
 
@@ -225,10 +225,10 @@ def solve_spd(
             f"backend {backend!r} is not provided here: this package only ships the B200 solver "
             "(use the reference's SciPy path for backend='cpu')"
         )
-    if preconditioner == "jacobi+learned":
+    if preconditioner in ("jacobi+learned", "block"):
         from .learned import solve_learned
 
-        return solve_learned(A, b, tol=tol, maxiter=maxiter, precision=precision, **kw)
+        return solve_learned(A, b, tol=tol, maxiter=maxiter, precision=precision, preconditioner=preconditioner, **kw)
     return solve_b200_cg(A, b, tol=tol, maxiter=maxiter, preconditioner=preconditioner, precision=precision, **kw)
 
 

@@ -42,6 +42,80 @@ def mode_inverses(M2, Qx2, Qy2, KN2, mu, sig, kap, a):
     return Ainv, Sinv
 
 
+def _dgemm_nt(lib, M, N, K, A, lda, sA, B, ldb, sB, s, sS, C, ldc, sC, batch, beta=0.0):
+    _lib.check(lib.cutcell_dgemm_nt(M, N, K, A.data_ptr(), lda, sA, B.data_ptr(), ldb, sB,
+                                    s.data_ptr() if s is not None else None, sS, beta, C.data_ptr(), ldc, sC, batch,
+                                    _lib.current_stream_ptr()), "cutcell_dgemm_nt")
+
+
+def mode_operators_gpu(M2, Qx2, Qy2, KN2, mu, sig, kap, a, device="cuda", timings=None):
+    """The per-mode operators of FastDiagHill::build (hill_fastdiag.h:26-43)
+    through one shared generalised eigenbasis instead of 2 nz dense
+    inversions of nr x nr matrices (the Lynch-Rice-Thomas form of
+    cpp/include/solvers/fastdiag3.h:29-92):
+
+    * KN2 Phi = M2 Phi diag(lam), Phi^T M2 Phi = I (host LAPACK, once), so
+      A_k = (mu_k + a sig_k) M2 + a mu_k KN2 = Phi^-T diag(c1 + c2 lam) Phi^-1
+      and A_k^{-1} = Phi diag(d_k) Phi^T, d_k = 1 / (c1_k + c2_k lam);
+    * with G = [Qx2 Phi | Qy2 Phi | M2 Phi] the Schur complement is
+      S_k = G diag(mu_k^2 d_k, mu_k^2 d_k, kap_k^2 d_k) G^T;
+    * modes k and nz - k share mu, sig and kap^2, so only nz/2 + 1 distinct
+      modes are built.
+    The products run on the device (cutcell_dgemm_nt, FP64 tensor cores);
+    each S_k is inverted on the host (LAPACK, symmetric).  Returns device
+    tensors Ainv, Sinv of shape (nz, nr, nr)."""
+    import time
+
+    import scipy.linalg
+    import torch
+
+    lib = _lib.load()
+    dv = torch.device(device)
+    f64 = torch.float64
+    T = {} if timings is None else timings
+    t0 = time.perf_counter()
+    M2 = np.asarray(M2, dtype=float)
+    KN2 = np.asarray(KN2, dtype=float)
+    lam, Phi = scipy.linalg.eigh(0.5 * (KN2 + KN2.T), 0.5 * (M2 + M2.T))
+    T["eigh_s"] = time.perf_counter() - t0
+    nr, nz = M2.shape[0], len(mu)
+    kd = np.arange(nz // 2 + 1)
+    c1 = np.asarray(mu)[kd] + a * np.asarray(sig)[kd]
+    c2 = a * np.asarray(mu)[kd]
+    d = 1.0 / (c1[:, None] + c2[:, None] * lam[None, :])  # (K, nr)
+    w = np.concatenate([(np.asarray(mu)[kd] ** 2)[:, None] * d, (np.asarray(mu)[kd] ** 2)[:, None] * d,
+                        (np.asarray(kap)[kd] ** 2)[:, None] * d], axis=1)  # (K, 3 nr)
+    t1 = time.perf_counter()
+    up = lambda x: torch.as_tensor(np.ascontiguousarray(x), dtype=f64).to(dv)
+    Phi_d, PhiT_d = up(Phi), up(Phi.T)
+    G = torch.empty((nr, 3 * nr), dtype=f64, device=dv)
+    for j, Op in enumerate((Qx2, Qy2, M2)):
+        Od = up(Op)
+        _dgemm_nt(lib, nr, nr, nr, Od, nr, 0, PhiT_d, nr, 0, None, 0, G[:, j * nr:], 3 * nr, 0, 1)
+    K = kd.size
+    d_d, w_d = up(d), up(w)
+    Ainv = torch.empty((nz, nr, nr), dtype=f64, device=dv)
+    _dgemm_nt(lib, nr, nr, nr, Phi_d, nr, 0, Phi_d, nr, 0, d_d, nr, Ainv, nr, nr * nr, K)
+    S = torch.empty((K, nr, nr), dtype=f64, device=dv)
+    _dgemm_nt(lib, nr, nr, 3 * nr, G, 3 * nr, 0, G, 3 * nr, 0, w_d, 3 * nr, S, nr, nr * nr, K)
+    torch.cuda.synchronize(dv)
+    T["device_gemm_s"] = time.perf_counter() - t1
+    T["device_gemm_flop"] = 2.0 * nr * nr * nr * 3 + 2.0 * nr * nr * nr * K + 2.0 * nr * nr * 3 * nr * K
+    t2 = time.perf_counter()
+    Sh = S.cpu().numpy()
+    Sinv = torch.empty((nz, nr, nr), dtype=f64, device=dv)
+    for k in range(K):
+        Sk = 0.5 * (Sh[k] + Sh[k].T)
+        Sinv[k].copy_(torch.as_tensor(np.linalg.inv(Sk)))
+    T["schur_inverse_s"] = time.perf_counter() - t2
+    for k in range(K, nz):  # modes nz - k
+        Ainv[k].copy_(Ainv[nz - k])
+        Sinv[k].copy_(Sinv[nz - k])
+    torch.cuda.synchronize(dv)
+    T["total_s"] = time.perf_counter() - t0
+    return Ainv, Sinv
+
+
 class FastDiagHill:
     def __init__(self, device="cuda"):
         import torch
@@ -50,15 +124,23 @@ class FastDiagHill:
         self._lib = _lib.load()
         self._ctx = None
 
-    def build(self, M2, Qx2, Qy2, KN2, Mz_row, Sz_row, Kz_row, a, *, inverses=None):
-        """Host build (FastDiagHill::build); ``inverses=(Ainv, Sinv)`` may be
-        supplied (host or device arrays) instead of being formed here."""
+    def build(self, M2, Qx2, Qy2, KN2, Mz_row, Sz_row, Kz_row, a, *, inverses=None, on_device: bool = False):
+        """FastDiagHill::build.  ``on_device=True`` forms the per-mode
+        operators through the shared eigenbasis on the device
+        (mode_operators_gpu); otherwise by dense host inversion as the
+        reference does.  ``inverses=(Ainv, Sinv)`` may be supplied instead."""
         import torch
 
         self.nr = int(M2.shape[0])
         self.nz = int(len(Mz_row))
         self.a = float(a)
         self.mu, self.sig, self.kap = z_symbols(Mz_row, Sz_row, Kz_row)
+        self.build_timings = {}
+        if inverses is None and on_device:
+            if KN2 is None:
+                raise ValueError("KN2 is needed to form the inverses")
+            inverses = mode_operators_gpu(M2, Qx2, Qy2, KN2, self.mu, self.sig, self.kap, float(a), self.device,
+                                          self.build_timings)
         if inverses is None:
             if KN2 is None:
                 raise ValueError("KN2 is needed to form the inverses")

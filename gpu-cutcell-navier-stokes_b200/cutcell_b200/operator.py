@@ -303,9 +303,8 @@ class CutCellOperator:
         if x is None:
             x = torch.empty_like(b)
         rep = _lib.CutcellReport()
-        pc = {"none": _lib.PRECOND_NONE, "jacobi": _lib.PRECOND_JACOBI, "jacobi+learned": _lib.PRECOND_JACOBI_LEARNED}[
-            preconditioner
-        ]
+        pc = {"none": _lib.PRECOND_NONE, "jacobi": _lib.PRECOND_JACOBI, "jacobi+learned": _lib.PRECOND_JACOBI_LEARNED,
+              "block": _lib.PRECOND_BLOCK}[preconditioner]
         _lib.check(
             self._lib.cutcell_pcg_solve(
                 self._ctx, b.data_ptr(), x.data_ptr(), float(tol), int(maxiter), _lib.PRECISIONS[precision], pc,

@@ -59,11 +59,17 @@ def _cached(key: str, builder) -> CutCellProblem:
     return prob
 
 
-def sphere_poisson(n: int = 32, p: int = 3, radius: float = 0.31, a_mass: float = 0.0, cache: bool = True):
+def sphere_poisson(n: int = 32, p: int = 3, radius: float = 0.31, a_mass: float = 0.0, cache: bool = True,
+                   native: bool | None = None):
+    """``native=False`` builds the cut quadrature in NumPy only (no
+    libcutcell_setup.so is loaded), cached under its own key."""
     u, f = manufactured_sine()
     phi = SphereExteriorLevelSet((0.5, 0.5, 0.5), radius)
-    build = lambda: build_problem(phi, n, p, a_mass=a_mass, forcing=f, dirichlet=u)
-    prob = _cached(_key(kind="sphere", n=n, p=p, r=radius, a=a_mass, v=2), build) if cache else build()
+    build = lambda: build_problem(phi, n, p, a_mass=a_mass, forcing=f, dirichlet=u, native=native)
+    key = dict(kind="sphere", n=n, p=p, r=radius, a=a_mass, v=2)
+    if native is False:
+        key["host"] = "numpy"
+    prob = _cached(_key(**key), build) if cache else build()
     ext = build_extension(prob.gamma, prob.basis, p)
     return prob, ext
 

@@ -37,7 +37,12 @@ enum {
 };
 
 enum { CUTCELL_FP64 = 0, CUTCELL_FP32_IR = 1, CUTCELL_BF16_IR = 2 };
-enum { CUTCELL_PRECOND_NONE = 0, CUTCELL_PRECOND_JACOBI = 1, CUTCELL_PRECOND_JACOBI_LEARNED = 2 };
+enum {
+    CUTCELL_PRECOND_NONE = 0,
+    CUTCELL_PRECOND_JACOBI = 1,
+    CUTCELL_PRECOND_JACOBI_LEARNED = 2, /* patch blocks where set, the network on the other patches */
+    CUTCELL_PRECOND_BLOCK = 3           /* patch blocks where set, Jacobi on the other patches */
+};
 
 typedef struct cutcell_ctx cutcell_ctx;
 
@@ -206,9 +211,19 @@ int cutcell_patch_targets(cutcell_ctx* ctx, const int32_t* patch_red, int32_t n_
 int cutcell_pcg_set_learned(cutcell_ctx* ctx, cutcell_mlp* mlp, const int32_t* patch_red, const float* patch_gamma,
                             int32_t n_patch);
 
-/* replace the network by exact patch inverses binv[n_patch][64][64] (block
- * Jacobi, the ceiling the network is trained towards); NULL restores the network */
+/* exact inverses binv[n_patch][64][64] (symmetric) on every patch of the
+ * attached layout (block Jacobi on all patches, the ceiling of patch-local
+ * corrections); NULL removes them */
 int cutcell_pcg_set_block_inverses(cutcell_ctx* ctx, const double* binv);
+/* Exact solves on chosen patches: slot[n_patch] is each patch's block in
+ * binv[n_blocks][64][64] (symmetric inverses of the patch blocks of E^T A E),
+ * or -1.  Used by CUTCELL_PRECOND_BLOCK (Jacobi on the patches without a
+ * block) and CUTCELL_PRECOND_JACOBI_LEARNED (the network on them); both run
+ * flexible PCG in FP64.  patch_red is the layout of cutcell_pcg_set_learned
+ * (the same pointer when a network is attached).  binv NULL removes the
+ * blocks.  All device pointers, kept by reference. */
+int cutcell_pcg_set_patch_blocks(cutcell_ctx* ctx, const int32_t* patch_red, int32_t n_patch, const int32_t* slot,
+                                 const double* binv);
 
 /* ---- periodic-hill fast diagonalisation (FastDiagHill, cpp/include/cut/hill_fastdiag.h:20-80) ----
  * create: the reduced 2D forms M2, Qx2, Qy2 (nr x nr, row-major), the z
@@ -223,6 +238,18 @@ int cutcell_fastdiag_create(int32_t nr, int32_t nz, const double* M2, const doub
 int cutcell_fastdiag_solve(cutcell_fastdiag* fd, const double* ux, const double* uy, const double* uz, double* ox,
                            double* oy, double* oz, void* stream);
 int cutcell_fastdiag_destroy(cutcell_fastdiag* fd);
+/* Batched FP64 GEMM on the FP64 tensor cores, the dense work of the
+ * fast-diagonalisation build through a shared generalised eigenbasis
+ * (the per-mode operators of FastDiagHill::build, hill_fastdiag.h:26-43, as
+ * A_k^-1 = Phi diag(d_k) Phi^T and S_k = G diag(w_k) G^T, the
+ * Lynch-Rice-Thomas form of cpp/include/solvers/fastdiag3.h:29-92):
+ *   C_b = A_b diag(s_b) B_b^T (+ beta C_b),  b = 0 .. batch-1,
+ * A_b (M x K) and B_b (N x K) row-major with leading dimensions lda, ldb; s
+ * (optional, NULL = ones) a K-vector per batch; strides in elements, 0 shares
+ * an operand; asynchronous on `stream`. */
+int cutcell_dgemm_nt(int32_t M, int32_t N, int32_t K, const double* A, int64_t lda, int64_t strideA, const double* B,
+                     int64_t ldb, int64_t strideB, const double* s, int64_t strideS, double beta, double* C, int64_t ldc,
+                     int64_t strideC, int32_t batch, void* stream);
 
 /* ---- periodic-hill advection and fast step ----
  * hill_skew_conv (cpp/include/cut/hill3d.h:519-538) for all three velocity

@@ -167,7 +167,7 @@ def read_reference_dump(path):
     return d
 
 
-def reference_dump(ne=3, nz=6, seed=99, steps=1, ref_root=None):
+def reference_dump(ne=3, nz=6, seed=99, steps=1, ref_root=None, physical=False):
     """Run the compiled reference (oracle/_ref/hill_ref; built from the
     reference's headers when the tree is present) and parse its dump.
     Returns None when the binary is unavailable."""
@@ -187,6 +187,6 @@ def reference_dump(ne=3, nz=6, seed=99, steps=1, ref_root=None):
         return None
     with tempfile.TemporaryDirectory() as td:
         out = Path(td) / "h.bin"
-        subprocess.run([str(exe), str(ne), str(nz), str(seed), str(out), str(steps)], check=True,
-                       capture_output=True)
+        subprocess.run([str(exe), str(ne), str(nz), str(seed), str(out), str(steps), str(int(physical))],
+                       check=True, capture_output=True)
         return read_reference_dump(out)

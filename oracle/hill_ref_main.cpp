@@ -5,7 +5,7 @@
 // doubles.  Test infrastructure: it generates the golden vectors that pin the
 // NumPy restatement (oracle/hill.py) and the device solve.
 //
-//   hill_ref <ne> <nz> <seed> <out.bin> [steps]
+//   hill_ref <ne> <nz> <seed> <out.bin> [steps] [physical]
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -17,15 +17,16 @@ static void put(FILE* f, const std::vector<double>& v) { fwrite(v.data(), sizeof
 
 int main(int argc, char** argv) {
     if (argc < 5) {
-        std::fprintf(stderr, "usage: hill_ref ne nz seed out.bin [steps]\n");
+        std::fprintf(stderr, "usage: hill_ref ne nz seed out.bin [steps] [physical]\n");
         return 2;
     }
     const int ne = std::atoi(argv[1]), nz = std::atoi(argv[2]), seed = std::atoi(argv[3]);
     const int steps = argc > 5 ? std::atoi(argv[5]) : 0;
+    const bool physical = argc > 6 && std::atoi(argv[6]) != 0;
     const int p = 3;
     const double Lz = 4.5, a = 0.01, dt = 0.02, fx = 0.7;
     Hill3D H;
-    H.build(ne, p, nz, Lz);
+    H.build(ne, p, nz, Lz, physical);
     FastDiagHill fd;
     fd.build(H, a);
     const int nr = fd.nr;

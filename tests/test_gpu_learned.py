@@ -64,28 +64,59 @@ def test_patch_layout_covers_reduced_dofs_once(torch_cuda):
     op.close()
 
 
-def test_learned_fcg_converges_to_fp64_solution(torch_cuda):
-    from cutcell_b200 import solve_spd
-    from cutcell_b200.learned import PatchMLP, attach, generate_pairs, train
-    from cutcell_b200.operator import CutCellOperator
+@pytest.mark.parametrize("n", [16, 24, 32])
+def test_learned_preconditioner_beats_jacobi(torch_cuda, n):
+    """Sphere r = 0.31, p = 3.  The network is trained (project kernels, BF16
+    weights) on solver-generated pairs of two other radii in [0.2, 0.4] and
+    used on the canonical patches; every other patch gets its exact block.
+    Asserts: fewer flexible-PCG iterations than plain Jacobi-PCG, no more
+    than the same split with Jacobi on the canonical patches (the method
+    without the network) plus one, and the FP64 solution's accuracy at tol
+    1e-11.  Prints the block-Jacobi ceiling (exact solves on every patch)
+    beside.  Where the grid has no canonical patch (small n) the network has
+    nothing to learn and the split is exact blocks everywhere."""
+    import torch
 
-    prob, ext, A_full, A_red, b = system("sphere", 9, 3)
+    from cutcell_b200 import solve_spd
+    from cutcell_b200.learned import PatchMLP, attach, attach_blocks, fit_linear, generate_pairs, train
+    from cutcell_b200.operator import CutCellOperator
+    from cutcell_b200.workloads import sphere_poisson
+
+    prob, ext = sphere_poisson(n, 3, 0.31)
+    b = np.asarray(ext.E.T @ prob.load)
     op = CutCellOperator(prob, ext)
-    net = PatchMLP(seed=1)
-    X, T = generate_pairs([op], 3000, seed=7)
-    hist = train(net, X, T, epochs=8, batch=256, lr=2e-3)
-    assert hist[-1] < hist[0]  # the network learns something
-    attach(op, net)
-    x, rep = solve_spd(op, b, tol=1e-9, maxiter=5000, preconditioner="jacobi+learned")
-    assert rep.success, rep
-    assert rep.relative_residual <= 1e-9
-    xd = spla.spsolve(A_red.tocsc(), b)
-    xp, rep_plain = solve_spd(op, b, tol=1e-9, maxiter=5000)
-    # the same relative residual as plain FP64 Jacobi-PCG; the error against
-    # the direct solution stays at the level the plain solve reaches
-    err = np.linalg.norm(x - xd) / np.linalg.norm(xd)
-    err_plain = np.linalg.norm(xp - xd) / np.linalg.norm(xd)
-    assert err <= max(10 * err_plain, 1e-7), (err, err_plain)
-    print(f"learned FCG iterations {rep.iterations} vs plain {rep_plain.iterations}; err {err:.2e} plain {err_plain:.2e}")
+    train_ops = [CutCellOperator(*sphere_poisson(n, 3, r)) for r in (0.23, 0.38)]
+    try:
+        X, T = generate_pairs(train_ops, 4000, seed=7)
+    except ValueError:  # no canonical patch on this grid: nothing for the network
+        X = T = None
+    net = None
+    if X is not None:
+        # least-squares start, then Adam with the project's training kernels
+        net = PatchMLP(fit_linear(X, T), activation="identity")
+        hist = train(net, X, T, epochs=4, batch=256, lr=1e-5)
+        assert hist[-1] <= 1e-3 * float((T.double() ** 2).mean()), hist
+    for o in train_ops:
+        o.close()
+    _, rj = solve_spd(op, b, tol=1e-9, maxiter=20000)
+    _, rc = solve_spd(op, b, tol=1e-9, maxiter=20000, preconditioner="block")
+    attach_blocks(op, "noncanonical")
+    xb, rb_ = op.solve_device(torch.as_tensor(b).cuda(), tol=1e-9, maxiter=20000, preconditioner="block")
+    if net is None:
+        it_l, ok_l = rb_.iterations, rb_.status == 0
+    else:
+        attach(op, net)
+        _, rl = solve_spd(op, b, tol=1e-9, maxiter=20000, preconditioner="jacobi+learned")
+        it_l, ok_l = rl.iterations, rl.success
+    assert rj.success and rc.success and ok_l and rb_.status == 0
+    print(f"n={n}: jacobi {rj.iterations}, blocks without network {rb_.iterations}, learned {it_l}, "
+          f"block-Jacobi ceiling {rc.iterations}, network on {0 if net is None else int(X.shape[0])} pairs")
+    assert it_l < rj.iterations
+    assert it_l <= rb_.iterations + 1
+    x13, r13 = solve_spd(op, b, tol=1e-13, maxiter=20000)
+    if net is not None:
+        x11, r11 = solve_spd(op, b, tol=1e-11, maxiter=20000, preconditioner="jacobi+learned")
+        assert r11.success, r11
+        assert np.linalg.norm(x11 - x13) / np.linalg.norm(x13) < 1e-7
+        net.close()
     op.close()
-    net.close()

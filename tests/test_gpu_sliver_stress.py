@@ -9,8 +9,9 @@ Every case, on the device: FP64 matrix-free Jacobi-PCG converges at tol 1e-9
 and 1e-13; the FP32 and BF16 operator forms (PCG with FP64 residual
 replacement) converge at tol 1e-9 with iteration counts within the stated
 factor of plain FP64's, and solved to tol 1e-11 they lie within 1e-7
-(relative L2) of the FP64 tol-1e-13 solution.  Every fifth case (and three
-fixed fractions 1e-5, 1e-3, 1e-1) is also pinned to the oracle on the CPU:
+(relative L2) of the FP64 tol-1e-13 solution.  Three fixed fractions 1e-5, 1e-3,
+1e-1 run too; cases 0, 12, 24 and the 1e-5 one are also pinned to the
+oracle on the CPU:
 the FP64 iterations are within max(1, 2 %) of the oracle CG's on the
 independently assembled E^T A E, and the FP64 tol-1e-13 solution is within
 1e-9 of the oracle's."""
@@ -32,10 +33,10 @@ ITER_FACTOR = {"fp32-ir": 1.35, "bf16-ir": 1.7}
 def _cases():
     from cutcell_b200.workloads import sliver_stress_cases
 
-    cases = [(f"cut{k}", nrm, eps, k % 5 == 0) for k, (nrm, eps) in enumerate(sliver_stress_cases(25))]
+    cases = [(f"cut{k}", nrm, eps, k % 12 == 0) for k, (nrm, eps) in enumerate(sliver_stress_cases(25))]
     rng = np.random.default_rng(12345)
     for j, eps in enumerate(FIXED):
-        cases.append((f"fixed{j}", np.abs(rng.standard_normal(3)) + 1e-3, eps, True))
+        cases.append((f"fixed{j}", np.abs(rng.standard_normal(3)) + 1e-3, eps, j == 0))
     return cases
 
 
