@@ -278,16 +278,13 @@ static int run_ru(cutcell_ctx* c, const OpHi& hi, const OpLo& lo, size_t smem, S
     return launch_coop(kern, *blocks, smem, s, hi, lo, a);
 }
 
+// Patch-preconditioned PCG (ppcg_kernel): mode 1 = exact blocks where set and
+// the network elsewhere, mode 2 = exact blocks where set and Jacobi elsewhere.
 template <class Op>
 static int run_fcg(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, cudaStream_t s, int* blocks,
                    int mode) {
-    auto kern = fcg_kernel<Op>;
     const size_t op_al = (op_smem + 15) & ~(size_t)15;
     const size_t smem = op_al + MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 3 * 64) * sizeof(float);
-    int st = ensure_part(c, kern, smem, blocks);
-    if (st) return st;
-    a.gs = make_gs(c, *blocks);
-    a.B = make_bufs(c);
     LearnedArgs L;
     memset(&L, 0, sizeof(L));
     if (mode == 1) L.W = c->mlp->weights();
@@ -295,6 +292,21 @@ static int run_fcg(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, c
     L.z = c->zl;
     L.rold = c->rold;
     L.use_mlp = mode;
+    L.ones = c->ones;
+    int st;
+    if (mode == 1) {
+        auto kern = ppcg_kernel<Op, true>;
+        st = ensure_part(c, kern, smem, blocks);
+        if (st) return st;
+        a.gs = make_gs(c, *blocks);
+        a.B = make_bufs(c);
+        return launch_coop(kern, *blocks, smem, s, op, a, L, op_al);
+    }
+    auto kern = ppcg_kernel<Op, false>;
+    st = ensure_part(c, kern, smem, blocks);
+    if (st) return st;
+    a.gs = make_gs(c, *blocks);
+    a.B = make_bufs(c);
     return launch_coop(kern, *blocks, smem, s, op, a, L, op_al);
 }
 

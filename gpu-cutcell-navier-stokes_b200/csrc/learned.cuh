@@ -327,7 +327,6 @@ __global__ void patch_targets_kernel(PatchMap pm, const double* e, const double*
 // Flexible PCG with the patch preconditioner z = M(r): exact patch blocks
 // where given, the network z = D^{-1} r + s * mlp(x) or Jacobi on the other
 // patches (Polak-Ribiere beta).
-// Safeguard: if r.z <= 0.1 * r.D^{-1}r the iteration uses Jacobi.
 // ---------------------------------------------------------------------------
 // Patch preconditioner modes (LearnedArgs::use_mlp):
 //   1: patches with an exact block use it, the others the network;
@@ -339,70 +338,101 @@ struct LearnedArgs {
     double* z;      // [n] preconditioned residual
     double* rold;   // [n]
     int use_mlp;
+    const double* ones;  // [n] ones: the fused p update p = 1 * z + beta p_old
 };
 
-// z_P = B_P^-1 r_P by one warp; B_P is symmetric, so lane l accumulates rows
-// l and l + 32 from the columns, each column one coalesced 512-byte read.
-__device__ __forceinline__ void patch_block_solve(const LearnedArgs& L, const PcgBufs& B, int k, int slot) {
+// One patch of the fused residual / preconditioner phase, by one warp: the
+// iterate and residual updates of the patch's DOFs (alpha = 0 at the start),
+// then z_P = M_P(r_P), and this lane's shares of r.z, r.r and r_old.z.
+template <bool kNet>
+__device__ __forceinline__ void patch_step(const LearnedArgs& L, const PcgBufs& B, int k, double alpha,
+                                           const double* pk, double* x, const MlpSmem& S, float* xs, double& rz,
+                                           double& rr, double& roz) {
     const int l = threadIdx.x & 31;
-    double rp0 = 0.0, rp1 = 0.0;
     const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
-    if (j0 >= 0) rp0 = __ldcg(B.r + j0);
-    if (j1 >= 0) rp1 = __ldcg(B.r + j1);
-    double z0 = 0.0, z1 = 0.0;
-    const double* Bk = L.pm.binv + (size_t)slot * 4096;
+    double ro0 = 0.0, ro1 = 0.0, r0 = 0.0, r1 = 0.0;
+    if (j0 >= 0) {
+        ro0 = B.r[j0];
+        r0 = ro0;
+        if (alpha != 0.0) {
+            x[j0] += alpha * __ldcg(pk + j0);
+            r0 = ro0 - alpha * __ldcg(B.Ap + j0);
+            B.r[j0] = r0;
+        }
+    }
+    if (j1 >= 0) {
+        ro1 = B.r[j1];
+        r1 = ro1;
+        if (alpha != 0.0) {
+            x[j1] += alpha * __ldcg(pk + j1);
+            r1 = ro1 - alpha * __ldcg(B.Ap + j1);
+            B.r[j1] = r1;
+        }
+    }
+    const int slot = (L.pm.binv && L.pm.slot) ? __ldg(L.pm.slot + k) : -1;
+    double z0, z1;
+    if (slot >= 0) {  // exact block solve, columns read coalesced (the inverse is symmetric)
+        const double* Bk = L.pm.binv + (size_t)slot * 4096;
+        z0 = 0.0;
+        z1 = 0.0;
 #pragma unroll 8
-    for (int q = 0; q < 64; ++q) {
-        const double rq = __shfl_sync(0xffffffffu, q < 32 ? rp0 : rp1, q & 31);
-        z0 += __ldg(Bk + q * 64 + l) * rq;
-        z1 += __ldg(Bk + q * 64 + l + 32) * rq;
+        for (int q = 0; q < 64; ++q) {
+            const double rq = __shfl_sync(0xffffffffu, q < 32 ? r0 : r1, q & 31);
+            z0 += __ldg(Bk + q * 64 + l) * rq;
+            z1 += __ldg(Bk + q * 64 + l + 32) * rq;
+        }
+    } else {
+        z0 = j0 >= 0 ? B.dinv[j0] * r0 : 0.0;
+        z1 = j1 >= 0 ? B.dinv[j1] * r1 : 0.0;
+        if constexpr (kNet) {
+            // network correction z += s (mlp(x) - mlp(-x)) / 2 from the features
+            // of the updated residual (the warp's own writes, ordered by syncwarp)
+            __syncwarp();
+            float* h1 = xs + MLP_IN;
+            float* h2 = h1 + 64;
+            float* y = h2 + 64;
+            const float s = patch_features_warp(L.pm, k, B.r, B.dinv, xs);
+            mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
+            const float yp0 = y[l], yp1 = y[l + 32];
+            __syncwarp();
+            xs[l] = -xs[l];
+            xs[l + 32] = -xs[l + 32];
+            xs[64 + l] = -xs[64 + l];
+            xs[64 + l + 32] = -xs[64 + l + 32];
+            __syncwarp();
+            mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
+            z0 += (double)s * (double)(0.5f * (yp0 - y[l]));
+            z1 += (double)s * (double)(0.5f * (yp1 - y[l + 32]));
+            __syncwarp();
+        }
     }
-    if (j0 >= 0) L.z[j0] = z0;
-    if (j1 >= 0) L.z[j1] = z1;
-}
-
-__device__ __forceinline__ void learned_precond_phase(const LearnedArgs& L, const PcgBufs& B, const MlpSmem& S,
-                                                      float* scratch) {
-    const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
-    float* xs = scratch + warp * (MLP_IN + 3 * 64);
-    float* h1 = xs + MLP_IN;
-    float* h2 = h1 + 64;
-    float* y = h2 + 64;
-    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
-    for (int k = gw; k < L.pm.n_patch; k += nw) {
-        const int slot = (L.pm.binv && L.pm.slot) ? __ldg(L.pm.slot + k) : -1;
-        if (slot >= 0) {
-            patch_block_solve(L, B, k, slot);
-            continue;
-        }
-        const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
-        if (L.use_mlp != 1) {  // block Jacobi: Jacobi on patches without a block
-            if (j0 >= 0) L.z[j0] = B.dinv[j0] * __ldcg(B.r + j0);
-            if (j1 >= 0) L.z[j1] = B.dinv[j1] * __ldcg(B.r + j1);
-            continue;
-        }
-        // odd part of the network in the residual: y = (f(u, g) - f(-u, g)) / 2,
-        // so the correction is linear under sign changes of r like the patch
-        // inverse it approximates
-        const float s = patch_features_warp(L.pm, k, B.r, B.dinv, xs);
-        mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
-        const float yp0 = y[l], yp1 = y[l + 32];
-        __syncwarp();
-        xs[l] = -xs[l];
-        xs[l + 32] = -xs[l + 32];
-        xs[64 + l] = -xs[64 + l];
-        xs[64 + l + 32] = -xs[64 + l + 32];
-        __syncwarp();
-        mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
-        const float ya = 0.5f * (yp0 - y[l]), yb = 0.5f * (yp1 - y[l + 32]);
-        if (j0 >= 0) L.z[j0] = B.dinv[j0] * __ldcg(B.r + j0) + (double)s * (double)ya;
-        if (j1 >= 0) L.z[j1] = B.dinv[j1] * __ldcg(B.r + j1) + (double)s * (double)yb;
-        __syncwarp();
+    if (j0 >= 0) {
+        L.z[j0] = z0;
+        rz += r0 * z0;
+        rr += r0 * r0;
+        roz += ro0 * z0;
+    }
+    if (j1 >= 0) {
+        L.z[j1] = z1;
+        rz += r1 * z1;
+        rr += r1 * r1;
+        roz += ro1 * z1;
     }
 }
 
-template <class Op>
-__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) fcg_kernel(Op op, SolveArgs a, LearnedArgs L, size_t op_smem) {
+// Patch-preconditioned flexible PCG (Polak-Ribiere beta) with the operator's
+// fused p update: per iteration
+//   apply:  p = z + beta p_old (phase 0 of the operator, z in place of D^-1 r
+//           and ones as the scale), A p, p.A p        (the operator's barriers)
+//   barrier, alpha = r.z / p.A p
+//   patch phase (one warp per patch): x += alpha p, r -= alpha A p,
+//           z = M(r) on the patch, partials of r.z, r.r, r_old.z
+//   barrier, rel = ||r|| / ||b||, beta = (r.z - r_old.z) / r.z_old
+// so an iteration takes the barriers of plain PCG.  Every reduced DOF lies in
+// exactly one patch.
+template <class Op, bool kNet>
+__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) ppcg_kernel(Op op, SolveArgs a, LearnedArgs L, size_t op_smem) {
+    static_assert(Op::kFusedP, "the patch PCG forms p inside the operator's first phase");
     extern __shared__ __align__(16) double sm[];
     __shared__ double sh[CUTCELL_WARPS + 1];
     char* smem_mlp = reinterpret_cast<char*>(sm) + op_smem;
@@ -410,12 +440,14 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) fcg_kernel(Op op, SolveArgs 
     const PcgBufs& B = a.B;
     const int n = B.n, nb = gridDim.x;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    const int warp = threadIdx.x >> 5;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
+    float* xs = scratch + warp * (MLP_IN + 3 * 64);
     double* part = B.part;
     const GridSync& gs = a.gs;
-    // network image loaded once; the operator's shared memory precedes it
     MlpSmem S;
-    if (L.use_mlp == 1) S = mlp_load_smem(L.W, smem_mlp);
-    // x = 0, r = b, z = M(r)
+    if constexpr (kNet) S = mlp_load_smem(L.W, smem_mlp);
+    // x = 0, r = b, ||b||
     double bb = 0.0;
     for (int i = gtid; i < n; i += gstride) {
         a.x[i] = 0.0;
@@ -429,30 +461,20 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) fcg_kernel(Op op, SolveArgs 
     if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
     double bnorm = sqrt(grid_reduce(part + 1 * nb, nb, sh));
     if (bnorm == 0.0) bnorm = 1.0;
-    if (L.use_mlp) learned_precond_phase(L, B, S, scratch);
-    if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
-    double rz = 0.0, rzj = 0.0;
-    for (int i = gtid; i < n; i += gstride) {
-        const double ri = B.r[i], zj = B.dinv[i] * ri;
-        const double zi = L.use_mlp ? __ldcg(L.z + i) : zj;
-        rz += ri * zi;
-        rzj += ri * zj;
-    }
+    // z = M(b), p = z, rz
+    double rz = 0.0, rr = 0.0, roz = 0.0;
+    for (int q = gw; q < L.pm.n_patch; q += nw) patch_step<kNet>(L, B, q, 0.0, B.p, a.x, S, xs, rz, rr, roz);
     rz = block_sum(rz, sh);
-    rzj = block_sum(rzj, sh);
-    if (threadIdx.x == 0) {
-        part[0 * nb + blockIdx.x] = rz;
-        part[6 * nb + blockIdx.x] = rzj;
-    }
+    if (threadIdx.x == 0) part[0 * nb + blockIdx.x] = rz;
     if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
     rz = grid_reduce(part + 0 * nb, nb, sh);
-    rzj = grid_reduce(part + 6 * nb, nb, sh);
-    bool jac = !L.use_mlp || !(rz > 0.1 * rzj);
-    if (jac) rz = rzj;
-    for (int i = gtid; i < n; i += gstride) B.p[i] = jac ? B.dinv[i] * B.r[i] : __ldcg(L.z + i);
+    for (int i = gtid; i < n; i += gstride) B.p[i] = __ldcg(L.z + i);
     if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
+    double* P[2] = {B.p, B.p2};
+    double beta = 0.0;
     for (k = 1; k <= a.maxiter && status != CUTCELL_E_BARRIER; ++k) {
-        double pap = op.apply(B.p, B.Ap, gs, sm);
+        double* pk = P[(k - 1) & 1];
+        double pap = (k > 1) ? op.apply_next(P[k & 1], pk, L.z, L.ones, beta, B.Ap, gs, sm) : op.apply(pk, B.Ap, gs, sm);
         if (grid_error(gs)) {
             status = CUTCELL_E_BARRIER;
             break;
@@ -469,22 +491,23 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) fcg_kernel(Op op, SolveArgs 
             break;
         }
         const double alpha = rz / pap;
-        double rr = 0.0;
-        for (int i = gtid; i < n; i += gstride) {
-            a.x[i] += alpha * B.p[i];
-            const double ro = B.r[i];
-            L.rold[i] = ro;
-            const double ri = ro - alpha * __ldcg(B.Ap + i);
-            B.r[i] = ri;
-            rr += ri * ri;
+        double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+        for (int q = gw; q < L.pm.n_patch; q += nw) patch_step<kNet>(L, B, q, alpha, pk, a.x, S, xs, d0, d1, d2);
+        d0 = block_sum(d0, sh);
+        d1 = block_sum(d1, sh);
+        d2 = block_sum(d2, sh);
+        if (threadIdx.x == 0) {
+            part[3 * nb + blockIdx.x] = d0;
+            part[4 * nb + blockIdx.x] = d1;
+            part[5 * nb + blockIdx.x] = d2;
         }
-        rr = block_sum(rr, sh);
-        if (threadIdx.x == 0) part[3 * nb + blockIdx.x] = rr;
         if (!grid_sync(gs)) {
             status = CUTCELL_E_BARRIER;
             break;
         }
-        rel = sqrt(grid_reduce(part + 3 * nb, nb, sh)) / bnorm;
+        const double rzn = grid_reduce(part + 3 * nb, nb, sh);
+        rel = sqrt(grid_reduce(part + 4 * nb, nb, sh)) / bnorm;
+        const double roz_n = grid_reduce(part + 5 * nb, nb, sh);
         if (!isfinite(rel)) {
             status = CUTCELL_E_NAN;
             break;
@@ -493,51 +516,8 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) fcg_kernel(Op op, SolveArgs 
             status = CUTCELL_OK;
             break;
         }
-        if (L.use_mlp) learned_precond_phase(L, B, S, scratch);
-        if (!grid_sync(gs)) {
-            status = CUTCELL_E_BARRIER;
-            break;
-        }
-        // rz_new = r.z, rzo = r_old.z (Polak-Ribiere), Jacobi versions for the safeguard
-        double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
-        for (int i = gtid; i < n; i += gstride) {
-            const double ri = B.r[i], ro = L.rold[i], zj = B.dinv[i] * ri;
-            const double zi = L.use_mlp ? __ldcg(L.z + i) : zj;
-            d0 += ri * zi;
-            d1 += ro * zi;
-            d2 += ri * zj;
-            d3 += ro * zj;
-        }
-        d0 = block_sum(d0, sh);
-        d1 = block_sum(d1, sh);
-        d2 = block_sum(d2, sh);
-        d3 = block_sum(d3, sh);
-        if (threadIdx.x == 0) {
-            part[4 * nb + blockIdx.x] = d0;
-            part[5 * nb + blockIdx.x] = d1;
-            part[6 * nb + blockIdx.x] = d2;
-            part[7 * nb + blockIdx.x] = d3;
-        }
-        if (!grid_sync(gs)) {
-            status = CUTCELL_E_BARRIER;
-            break;
-        }
-        d0 = grid_reduce(part + 4 * nb, nb, sh);
-        d1 = grid_reduce(part + 5 * nb, nb, sh);
-        d2 = grid_reduce(part + 6 * nb, nb, sh);
-        d3 = grid_reduce(part + 7 * nb, nb, sh);
-        jac = !L.use_mlp || !(d0 > 0.1 * d2);
-        const double rzn = jac ? d2 : d0;
-        const double beta = (rzn - (jac ? d3 : d1)) / rz;
+        beta = (rzn - roz_n) / rz;
         rz = rzn;
-        for (int i = gtid; i < n; i += gstride) {
-            const double zi = jac ? B.dinv[i] * B.r[i] : __ldcg(L.z + i);
-            B.p[i] = zi + beta * B.p[i];
-        }
-        if (!grid_sync(gs)) {
-            status = CUTCELL_E_BARRIER;
-            break;
-        }
     }
     const int iters = k > a.maxiter ? a.maxiter : k;
     double true_rel = -1.0;
@@ -552,3 +532,4 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) fcg_kernel(Op op, SolveArgs 
         a.res->true_rel = true_rel;
     }
 }
+

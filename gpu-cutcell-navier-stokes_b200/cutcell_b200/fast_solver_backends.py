@@ -182,9 +182,11 @@ def solve_b200_cg(
     b_np = np.asarray(b, dtype=float)
     t0 = perf_counter()
     own = False
-    if isinstance(A, (CutCellOperator, CsrDeviceMatrix)):
+    if isinstance(A, (CutCellOperator, CsrDeviceMatrix)) or (hasattr(A, "solve_device") and hasattr(A, "n")):
+        # device-resident operators (matrix-free tiles, CSR, Kronecker cut boxes)
         dev_op = A
-        method = "b200-matrix-free-pcg" if isinstance(A, CutCellOperator) else "b200-csr-pcg"
+        method = getattr(A, "method", None) or ("b200-matrix-free-pcg" if isinstance(A, CutCellOperator)
+                                                else "b200-csr-pcg")
     else:
         dev_op = CsrDeviceMatrix(A, device=device)
         own = True

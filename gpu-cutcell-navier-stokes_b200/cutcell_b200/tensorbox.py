@@ -335,6 +335,8 @@ class KronOperator:
     context of kind KRON).  ``solve_device`` solves with the SPD Poisson form
     A; ``apply(x, form)`` applies any of A, H, K, Qx, Qy, Qz, Sx, Sy, Sz."""
 
+    method = "b200-matrix-free-kron-pcg"
+
     def __init__(self, box: CutBox, device="cuda"):
         import torch
 

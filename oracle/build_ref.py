@@ -39,5 +39,28 @@ def build(ref_root: str | None = None) -> Path | None:
     return out
 
 
+def build_gpu_run(ref_root: str | None = None) -> Path | None:
+    """The reference's own device hill step (cpp/gpu/gpu_run.cu: its kernels
+    plus cuBLAS, the baseline GPU time of hill_fastdiag_step), compiled from
+    that one source file with nvcc for sm_100a into oracle/_ref/gpu_run."""
+    import shutil
+
+    root = reference_root(ref_root)
+    src = root / "cpp" / "gpu" / "gpu_run.cu"
+    inc = root / "cpp" / "include"
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not src.exists() or not Path(nvcc).exists():
+        return None
+    out = HERE / "_ref" / "gpu_run"
+    out.parent.mkdir(exist_ok=True)
+    if out.exists() and out.stat().st_mtime >= src.stat().st_mtime:
+        return out
+    cmd = [nvcc, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+           *[f"-I{inc / d}" for d in ("core", "operators", "solvers", "cut", "io")], str(src), "-lcublas", "-o", str(out)]
+    subprocess.run(cmd, check=True, capture_output=True)
+    return out
+
+
 if __name__ == "__main__":
     print(build(*sys.argv[1:]))
+    print(build_gpu_run(*sys.argv[1:]))

@@ -6,6 +6,7 @@
 // NumPy restatement (oracle/hill.py) and the device solve.
 //
 //   hill_ref <ne> <nz> <seed> <out.bin> [steps] [physical]
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -96,7 +97,10 @@ int main(int argc, char** argv) {
     }
     if (steps > 0) {
         HillNS st = s;
+        const auto t0 = std::chrono::steady_clock::now();
         for (int k = 0; k < steps; ++k) hill_fastdiag_step(H, fd, st, dt, fx);
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "step_ms=%.3f\n", ms / steps);
         put(f, st.ux.v);
         put(f, st.uy.v);
         put(f, st.uz.v);

@@ -152,7 +152,8 @@ def test_matrix_free_pcg_matches_oracle(torch_cuda, kind, n, p):
     for prec in ("fp32-ir", "bf16-ir"):
         x3, rep3 = solve_spd(op_, b, tol=1e-9, maxiter=20000, precision=prec)
         assert rep3.success, (prec, rep3)
-        assert rep3.relative_residual <= 1e-8 and rep3.iterations <= 1.3 * rep.iterations + 5, (prec, rep3, rep)
+        factor = {"fp32-ir": 1.35, "bf16-ir": 1.7}[prec]  # as in the sliver-stress set
+        assert rep3.relative_residual <= 1e-8 and rep3.iterations <= factor * rep.iterations + 5, (prec, rep3, rep)
         x4, rep4 = solve_spd(op_, b, tol=1e-11, maxiter=20000, precision=prec)
         assert rep4.success, (prec, rep4)
         assert np.linalg.norm(x4 - xd) / np.linalg.norm(xd) < 1e-7

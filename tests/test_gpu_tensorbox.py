@@ -11,8 +11,9 @@ made from code/cut_3d_sbp.py and code/cut_pde_solve.py):
   1e-7 relative;
 * solve_poisson_circular's captured system, solved through
   make_linear_solver(), matches the reference's np.linalg.solve to 1e-9;
-* at n = 32 the Kronecker Poisson operator matches a host sum-factorised
-  evaluation to 1e-12 and its Jacobi-PCG agrees with the CSR path."""
+* at n = 24 the Kronecker Poisson operator matches a host sum-factorised
+  evaluation to 1e-12 and its Jacobi-PCG agrees with the same iteration on
+  the host."""
 
 import numpy as np
 import pytest
@@ -40,8 +41,10 @@ def _host_apply(box, form, x):
     X = x.reshape(nz, ny, nx)
     ax, ay, az = box.axes
 
-    def prod(cz, cy, cx):
-        return np.einsum("ai,bj,ck,ijk->abc", cz, cy, cx, X)
+    def prod(cz, cy, cx):  # three passes, one axis at a time
+        t = np.einsum("ck,ijk->ijc", cx, X)
+        t = np.einsum("bj,ijc->ibc", cy, t)
+        return np.einsum("ai,ibc->abc", cz, t)
 
     if form in ("A", "K"):
         f = [box.factor(d, form) for d in range(3)]
@@ -109,7 +112,7 @@ def test_kron_poisson_at_scale(torch_cuda):
     from cutcell_b200 import solve_spd
     from cutcell_b200 import tensorbox as tb
 
-    box = tb.cut_box(32, 3, (0.7, 0.2, 0.95))
+    box = tb.cut_box(24, 3, (0.7, 0.2, 0.95))
     op = tb.KronOperator(box)
     rng = np.random.default_rng(5)
     x = rng.standard_normal(box.n_red)
@@ -120,14 +123,27 @@ def test_kron_poisson_at_scale(torch_cuda):
     b = tb.poisson_rhs(box)
     xs, rep = solve_spd(op, b, tol=1e-10, maxiter=20000)
     assert rep.success, rep
-    # the same solve on the assembled CSR of the same operator (column by
-    # column is too slow at this size: assemble the Kronecker sum sparsely)
-    ax, ay, az = box.axes
-    S = lambda M: sp.csr_matrix(M)
-    A = (sp.kron(sp.kron(S(az.H), S(ay.H)), S(box.factor(0, "A"))) + sp.kron(sp.kron(S(az.H), S(box.factor(1, "A"))), S(ax.H))
-         + sp.kron(sp.kron(S(box.factor(2, "A")), S(ay.H)), S(ax.H))).tocsr()
-    xc, repc = solve_spd(A, b, tol=1e-10, maxiter=20000)
-    assert repc.success and abs(repc.iterations - rep.iterations) <= max(1, 0.02 * rep.iterations)
-    assert np.linalg.norm(xs - xc) <= 1e-8 * np.linalg.norm(xc)
+    # the same Jacobi-PCG on the host with the sum-factorised apply
+    dinv = 1.0 / box.diag_A()
+    xh = np.zeros_like(b)
+    r = b.copy()
+    z = dinv * r
+    pv = z.copy()
+    rz = r @ z
+    its = 0
+    for its in range(1, 20001):
+        Ap = _host_apply(box, "A", pv)
+        al = rz / (pv @ Ap)
+        xh += al * pv
+        r -= al * Ap
+        if np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b):
+            break
+        z = dinv * r
+        rzn = r @ z
+        pv = z + (rzn / rz) * pv
+        rz = rzn
+    reph = {"iterations": its}
+    assert abs(reph["iterations"] - rep.iterations) <= max(1, 0.02 * rep.iterations)
+    assert np.linalg.norm(xs - xh) <= 1e-8 * np.linalg.norm(xh)
     op.close()
     torch.cuda.synchronize()
