@@ -227,14 +227,24 @@ def manufactured_3d():
     return u, f, grad
 
 
+# Every multi-operand contraction here runs with optimize=True: NumPy then
+# contracts one axis at a time through BLAS; without it a four-operand einsum
+# is a single loop over all six indices (~1e11 operations at n = 24).
+
+
 def poisson_rhs(box: CutBox) -> np.ndarray:
     """Reduced load: volume term int f phi plus the face terms
     int_F g (beta phi - dn phi), g = u, on all six faces, pulled back by E."""
-    u, f, _ = manufactured_3d()
+    u, _, _ = manufactured_3d()
     quads = [cut_interval_quadrature(box.basis, a.left) for a in box.axes]
     (x, wx, Vx, _), (y, wy, Vy, _), (z, wz, Vz, _) = quads
-    F = f(x[:, None, None], y[None, :, None], z[None, None, :])
-    b = np.einsum("ip,jq,kr,pqr->ijk", Vx * wx, Vy * wy, Vz * wz, F)  # (x, y, z)
+    # f = -(0.36 - 2 pi^2) exp(0.6 x) cos(pi y) sin(pi z) is a product of 1D
+    # factors, so its tensor-quadrature moments are an outer product of three
+    # 1D moments (no n_q^3 grid: 512^3 points at n = 64)
+    mx = Vx @ (wx * np.exp(0.6 * x))
+    my = Vy @ (wy * np.cos(pi * y))
+    mz = Vz @ (wz * np.sin(pi * z))
+    b = -(0.36 - 2.0 * pi * pi) * mx[:, None, None] * my[None, :, None] * mz[None, None, :]  # (x, y, z)
     lefts = [a.left for a in box.axes]
     for d in range(3):
         o = [j for j in range(3) if j != d]
@@ -243,7 +253,7 @@ def poisson_rhs(box: CutBox) -> np.ndarray:
             cg = [quads[0][0], quads[1][0], quads[2][0]]
             cg[d] = np.array([coord])
             G = np.squeeze(u(cg[0][:, None, None], cg[1][None, :, None], cg[2][None, None, :]), axis=d)
-            fc = np.einsum("ip,jq,pq->ij", quads[o[0]][2] * quads[o[0]][1], quads[o[1]][2] * quads[o[1]][1], G)
+            fc = np.einsum("ip,jq,pq->ij", quads[o[0]][2] * quads[o[0]][1], quads[o[1]][2] * quads[o[1]][1], G, optimize=True)
             v = box.beta * trace - sign * dtrace
             if d == 0:
                 b += np.einsum("a,bc->abc", v, fc)
@@ -253,7 +263,7 @@ def poisson_rhs(box: CutBox) -> np.ndarray:
                 b += np.einsum("c,ab->abc", v, fc)
     ax, ay, az = box.axes
     full = np.transpose(b, (2, 1, 0))  # (z, y, x): x fastest
-    return np.einsum("zk,yj,xi,zyx->kji", az.E, ay.E, ax.E, full).reshape(-1)
+    return np.einsum("zk,yj,xi,zyx->kji", az.E, ay.E, ax.E, full, optimize=True).reshape(-1)
 
 
 def poisson_errors(box: CutBox, coeff_red: np.ndarray) -> dict:
@@ -263,20 +273,34 @@ def poisson_errors(box: CutBox, coeff_red: np.ndarray) -> dict:
     ax, ay, az = box.axes
     nx, ny, nz = box.shape
     c = coeff_red.reshape(nz, ny, nx)
-    alpha = np.einsum("zk,yj,xi,kji->zyx", az.E, ay.E, ax.E, c)
+    alpha = np.einsum("zk,yj,xi,kji->zyx", az.E, ay.E, ax.E, c, optimize=True)
     (x, wx, Vx, dVx), (y, wy, Vy, dVy), (z, wz, Vz, dVz) = [cut_interval_quadrature(box.basis, a.left) for a in box.axes]
-    uh = np.einsum("zyx,xp,yq,zr->pqr", alpha, Vx, Vy, Vz)
-    gx = np.einsum("zyx,xp,yq,zr->pqr", alpha, dVx, Vy, Vz)
-    gy = np.einsum("zyx,xp,yq,zr->pqr", alpha, Vx, dVy, Vz)
-    gz = np.einsum("zyx,xp,yq,zr->pqr", alpha, Vx, Vy, dVz)
-    W = wx[:, None, None] * wy[None, :, None] * wz[None, None, :]
-    X, Y, Z = x[:, None, None], y[None, :, None], z[None, None, :]
-    ue = u(X, Y, Z)
-    ex, ey, ez = grad(X, Y, Z)
-    l2 = np.sqrt(np.sum(W * (uh - ue) ** 2)) / np.sqrt(np.sum(W * ue**2))
-    h1 = np.sqrt(np.sum(W * ((gx - ex) ** 2 + (gy - ey) ** 2 + (gz - ez) ** 2))) / np.sqrt(
-        np.sum(W * (ex**2 + ey**2 + ez**2)))
-    linf = np.max(np.abs(uh - ue)) / np.max(np.abs(ue))
+    # y and z contracted once; the x contraction and the error sums run over
+    # slabs of x quadrature points so the n_q^3 grid is never held whole
+    t_vv = np.einsum("zyx,yq,zr->xqr", alpha, Vy, Vz, optimize=True)
+    t_dv = np.einsum("zyx,yq,zr->xqr", alpha, dVy, Vz, optimize=True)
+    t_vd = np.einsum("zyx,yq,zr->xqr", alpha, Vy, dVz, optimize=True)
+    nqx = x.size
+    sums = np.zeros(4)  # sum W (uh - u)^2, W u^2, W |grad uh - grad u|^2, W |grad u|^2
+    linf_num = linf_den = 0.0
+    slab = 32
+    for p0 in range(0, nqx, slab):
+        sl = slice(p0, min(p0 + slab, nqx))
+        uh = np.tensordot(Vx[:, sl], t_vv, axes=(0, 0))
+        gx = np.tensordot(dVx[:, sl], t_vv, axes=(0, 0))
+        gy = np.tensordot(Vx[:, sl], t_dv, axes=(0, 0))
+        gz = np.tensordot(Vx[:, sl], t_vd, axes=(0, 0))
+        W = wx[sl, None, None] * wy[None, :, None] * wz[None, None, :]
+        X, Y, Z = x[sl, None, None], y[None, :, None], z[None, None, :]
+        ue = u(X, Y, Z)
+        ex, ey, ez = grad(X, Y, Z)
+        sums += [np.sum(W * (uh - ue) ** 2), np.sum(W * ue**2),
+                 np.sum(W * ((gx - ex) ** 2 + (gy - ey) ** 2 + (gz - ez) ** 2)), np.sum(W * (ex**2 + ey**2 + ez**2))]
+        linf_num = max(linf_num, float(np.max(np.abs(uh - ue))))
+        linf_den = max(linf_den, float(np.max(np.abs(ue))))
+    l2 = np.sqrt(sums[0]) / np.sqrt(sums[1])
+    h1 = np.sqrt(sums[2]) / np.sqrt(sums[3])
+    linf = linf_num / linf_den
     return {"relative_l2_error": float(l2), "relative_h1_error": float(h1), "relative_linf_error": float(linf)}
 
 

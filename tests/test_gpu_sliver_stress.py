@@ -6,14 +6,17 @@ sides with the reference stress driver's seed rule 12345 + 17 n + p
 (code/fast_solver_workbench.py:167).
 
 Every case, on the device: FP64 matrix-free Jacobi-PCG converges at tol 1e-9
-and 1e-13; the FP32 and BF16 operator forms (PCG with FP64 residual
+and 1e-12; the FP32 and BF16 operator forms (PCG with FP64 residual
 replacement) converge at tol 1e-9 with iteration counts within the stated
 factor of plain FP64's, and solved to tol 1e-11 they lie within 1e-7
-(relative L2) of the FP64 tol-1e-13 solution.  Three fixed fractions 1e-5, 1e-3,
+(relative L2) of the FP64 tol-1e-12 solution.  (tol 1e-12, not 1e-13: success
+means a TRUE relative residual <= 10 tol, and on the 1e-5 slivers the FP64
+true-residual floor lies between 1e-12 and 1e-11 while the recursive one
+still falls below 1e-13.)  Three fixed fractions 1e-5, 1e-3,
 1e-1 run too; cases 0, 12, 24 and the 1e-5 one are also pinned to the
 oracle on the CPU:
 the FP64 iterations are within max(1, 2 %) of the oracle CG's on the
-independently assembled E^T A E, and the FP64 tol-1e-13 solution is within
+independently assembled E^T A E, and the FP64 tol-1e-12 solution is within
 1e-9 of the oracle's."""
 
 from __future__ import annotations
@@ -75,7 +78,7 @@ def test_sliver_stress_mixed_precision(torch_cuda, name, nrm, eps, pinned):
     try:
         x, rep = solve_spd(op, b, tol=1e-9, maxiter=50000)
         assert rep.success, rep
-        x64, rep64 = solve_spd(op, b, tol=1e-13, maxiter=50000)
+        x64, rep64 = solve_spd(op, b, tol=1e-12, maxiter=50000)
         assert rep64.success, rep64
         its = {"fp64": rep.iterations}
         for prec in ("fp32-ir", "bf16-ir"):
@@ -96,7 +99,7 @@ def test_sliver_stress_mixed_precision(torch_cuda, name, nrm, eps, pinned):
             A = restrict_spd(assemble_full(prob), ext.E).tocsr()
             _, rep_o = cg_loop(A, b, tol=1e-9, maxiter=50000)
             assert abs(rep.iterations - rep_o["iterations"]) <= max(1, 0.02 * rep_o["iterations"])
-            x_ref, _ = cg_loop(A, b, tol=1e-13, maxiter=50000)
+            x_ref, _ = cg_loop(A, b, tol=1e-12, maxiter=50000)
             assert np.linalg.norm(x64 - x_ref) / np.linalg.norm(x_ref) < 1e-9
     finally:
         op.close()
