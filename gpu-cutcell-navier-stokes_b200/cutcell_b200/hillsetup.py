@@ -588,8 +588,10 @@ def parabolic_ic(hs: HillSetup, *, ub: float = 1.0, amp: float = 0.01, seed: int
     hb = hs.wall.hbar(hs.xq)
     eta = np.clip((hs.yq - hb) / np.maximum(1.0 - hb, 1e-300), 0.0, 1.0)
     prof = 6.0 * ub * eta * (1.0 - eta)
-    fq = np.repeat(prof[:, None], hs.nzq, axis=1)
-    ux = l2_project(hs, fq)
+    # the profile is constant in z, so its z load is one row (wz^T Vz) and
+    # the projection is separable: no (n2q, nzq) field is formed
+    red = hs.phi.T @ (hs.w2 * prof)
+    ux = np.outer(hs.M2inv @ red, hs.Mzinv @ (hs.wz @ hs.Vz))
     rng = np.random.default_rng(seed)
     shape = (hs.nr, hs.nz)
     ux = ux + amp * ub * rng.uniform(-0.5, 0.5, shape)

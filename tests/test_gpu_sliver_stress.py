@@ -9,10 +9,13 @@ Every case, on the device: FP64 matrix-free Jacobi-PCG converges at tol 1e-9
 and 1e-12; the FP32 and BF16 operator forms (PCG with FP64 residual
 replacement) converge at tol 1e-9 with iteration counts within the stated
 factor of plain FP64's, and solved to tol 1e-11 they lie within 1e-7
-(relative L2) of the FP64 tol-1e-12 solution.  (tol 1e-12, not 1e-13: success
-means a TRUE relative residual <= 10 tol, and on the 1e-5 slivers the FP64
-true-residual floor lies between 1e-12 and 1e-11 while the recursive one
-still falls below 1e-13.)  Three fixed fractions 1e-5, 1e-3,
+(relative L2) of the FP64 tol-1e-12 solution.  The FP64 tol-1e-12 solve is
+checked by its recursive residual reaching tol ("converged") and its true
+relative residual reaching the floor bound 1e-10, not by ``success`` (a TRUE
+residual <= 10 tol): the true residual stops at its rounding floor, between
+1e-12 and 1.2e-11 on this set (cut19, 7,500 unknowns needing 7,200 Jacobi-CG
+iterations at 1e-9, floors at 1.1e-11, and so does the oracle's CG on the
+assembled matrix).  Three fixed fractions 1e-5, 1e-3,
 1e-1 run too; cases 0, 12, 24 and the 1e-5 one are also pinned to the
 oracle on the CPU:
 the FP64 iterations are within max(1, 2 %) of the oracle CG's on the
@@ -79,7 +82,7 @@ def test_sliver_stress_mixed_precision(torch_cuda, name, nrm, eps, pinned):
         x, rep = solve_spd(op, b, tol=1e-9, maxiter=50000)
         assert rep.success, rep
         x64, rep64 = solve_spd(op, b, tol=1e-12, maxiter=50000)
-        assert rep64.success, rep64
+        assert rep64.message == "converged" and rep64.relative_residual <= 1e-10, rep64
         its = {"fp64": rep.iterations}
         for prec in ("fp32-ir", "bf16-ir"):
             _, r9 = solve_spd(op, b, tol=1e-9, maxiter=50000, precision=prec)
