@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--p", type=int, default=3)
     ap.add_argument("--radius", type=float, default=0.31)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--variants", default="fp64,fp32-ir,bf16-ir,block,learned")
+    ap.add_argument("--variants", default="fp64,fp32-ir,bf16-ir,block,learned,twolevel")
     ap.add_argument("--no-extras", action="store_true", help="skip the batch / hill-step / cut-box summaries of the default run")
     ap.add_argument("--train-geometries", type=int, default=3)
     ap.add_argument("--train-pairs", type=int, default=20000)
@@ -740,9 +740,20 @@ def main():
                         "target_mean_square": float((T.double() ** 2).mean()), "train_s": time.perf_counter() - t0,
                         "canonical_patches": int(op._patch_solves.canonical.sum()) if hasattr(op, "_patch_solves") else None}
     t_blocks = None
+    t_coarse = None
     for prec in wanted:
         solve_kw = {"precision": prec}
-        if prec in ("learned", "block"):
+        if prec == "twolevel":
+            from cutcell_b200.coarse import attach_coarse
+            from cutcell_b200.learned import attach_blocks
+
+            attach_blocks(op, "all")
+            t0 = time.perf_counter()
+            cl = attach_coarse(op)
+            t_coarse = {"setup_s": time.perf_counter() - t0, "galerkin_s": cl.galerkin_s, "factor": cl.factor,
+                        "coarse_dofs": int(cl.keep.size), "minv_bytes": int(8 * cl.ncg * cl.ncg)}
+            solve_kw = {"precision": "fp64", "preconditioner": "twolevel"}
+        elif prec in ("learned", "block"):
             from cutcell_b200.learned import attach_blocks
 
             t0 = time.perf_counter()
@@ -806,6 +817,8 @@ def main():
         e2e_kw = {"preconditioner": "jacobi+learned"}
     elif e2e_prec == "block":
         e2e_kw = {"preconditioner": "block"}
+    elif e2e_prec == "twolevel":
+        e2e_kw = {"preconditioner": "twolevel"}
     for _ in range(2):
         solve_spd(op, b_pin.numpy(), tol=TOL, maxiter=20000, **e2e_kw)
     barrier()
@@ -870,6 +883,8 @@ def main():
         line["config"]["cpu_rel_err_vs_gpu_fp64"] = float(np.linalg.norm(xc - ref_x) / np.linalg.norm(xc))
     if t_blocks is not None:
         line["config"]["patch_blocks_setup_s"] = t_blocks
+    if t_coarse is not None:
+        line["config"]["coarse_level"] = t_coarse
     if world == 1 and not args.no_extras:
         line["extras"] = extras_summary(args, rank, world, local)
     if rank == 0:

@@ -1,0 +1,321 @@
+// Two-level patch preconditioner inside the persistent flexible PCG:
+//
+//   z = zc + B (r - A zc),   zc = P Ac^-1 P^T r,   Ac = P^T A P,
+//
+// B the exact 4x4x4 patch solves (Jacobi on patches without a stored block),
+// P the uniform B-spline refinement (knot insertion) from n / c to n elements
+// per axis, restricted to the rows of the reduced (kept) DOFs, and Ac its
+// Galerkin coarse operator, inverted densely on the host (a few thousand
+// coarse DOFs, read from L2 every iteration).  Coarse correction first, patch
+// solves on the corrected residual: the two-grid cycle without pre-smoothing.
+//
+// The tensor structure of P is used in both directions:
+//   restriction  P^T r : the x-contraction is fused into the x / r update
+//                        (one warp per x-line of the background grid), the
+//                        y-z contraction is one warp per coarse DOF;
+//   prolongation P y   : each reduced DOF sums its <= pw^3 coarse terms from
+//                        the coarse vector staged in shared memory, fused into
+//                        phase 0 of the apply A zc (its small rows of E zc are
+//                        formed from the same formula).
+// Every sum has a fixed order; results are bit-reproducible.
+#pragma once
+
+#include "learned.cuh"
+
+struct CoarseDev {
+    int nb, nbc, ncg;           // fine / coarse DOFs per axis, nbc^3
+    int pw, rw;                 // band widths of the prolongation rows / restriction rows
+    const int* plo;             // [nb] first coarse index of fine row x (plo + pw <= nbc)
+    const double* pval;         // [nb][pw]
+    const int* rlo;             // [nbc] first fine index of coarse column a (rlo + rw <= nb)
+    const double* rval;         // [nbc][rw]
+    const double* minv;         // [ncg][ncg] Ac^-1, zero rows / columns for coarse DOFs without fluid
+    double* t1;                 // [nb * nb][nbc] x-contracted residual, line (z, y) major
+    double* rc;                 // [ncg] P^T r
+    double* yc;                 // [ncg] Ac^-1 P^T r
+    double* zc;                 // [n] P yc
+    double* azc;                // [n] A zc
+};
+
+// zc_j = (P yc)_j from the coarse vector in shared memory
+struct ProlongFn {
+    CoarseDev cd;
+    const int* full_of_red;
+    const double* ys;
+    __device__ __forceinline__ double operator()(int j) const {
+        const int f = __ldg(full_of_red + j), nb = cd.nb, nbc = cd.nbc, pw = cd.pw;
+        const int x = f % nb, y = (f / nb) % nb, z = f / (nb * nb);
+        const int xl = __ldg(cd.plo + x), yl = __ldg(cd.plo + y), zl = __ldg(cd.plo + z);
+        double s = 0.0;
+        for (int tz = 0; tz < pw; ++tz) {
+            const double wz = __ldg(cd.pval + z * pw + tz);
+            const int cz = zl + tz;
+            if (wz == 0.0 || cz < 0 || cz >= nbc) continue;
+            for (int ty = 0; ty < pw; ++ty) {
+                const double wy = __ldg(cd.pval + y * pw + ty);
+                const int cy = yl + ty;
+                if (wy == 0.0 || cy < 0 || cy >= nbc) continue;
+                const double* row = ys + ((size_t)cz * nbc + cy) * nbc;
+                double sx = 0.0;
+                for (int tx = 0; tx < pw; ++tx) {
+                    const int cx = xl + tx;
+                    if (cx >= 0 && cx < nbc) sx += __ldg(cd.pval + x * pw + tx) * row[cx];
+                }
+                s += wz * wy * sx;
+            }
+        }
+        return s;
+    }
+};
+
+// x-lines of the background grid, one warp each: x += alpha p, r_old = r,
+// r -= alpha A p on the line's reduced DOFs (alpha = 0: r_old = r only), this
+// lane's share of r.r, and t1[line][a] = sum_x R[a][x] r(x) (zero off the
+// reduced DOFs).  lbuf: nb doubles of this warp's shared memory.
+__device__ __forceinline__ void tl_update_lines(const CoarseDev& cd, const ExtDev& ext, const PcgBufs& B, double* rold,
+                                                double alpha, const double* pk, double* x, double* lbuf, double& rr) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int nb = cd.nb, nbc = cd.nbc, rw = cd.rw;
+    for (int line = gw; line < nb * nb; line += nw) {
+        const size_t base = (size_t)line * nb;
+        for (int xi = lane; xi < nb; xi += 32) {
+            const int j = __ldg(ext.red_of_full + base + xi);
+            double rv = 0.0;
+            if (j >= 0) {
+                const double ro = __ldcg(B.r + j);
+                rv = ro;
+                if (alpha != 0.0) {
+                    x[j] += alpha * __ldcg(pk + j);
+                    rv = ro - alpha * __ldcg(B.Ap + j);
+                    B.r[j] = rv;
+                }
+                rold[j] = ro;
+                rr += rv * rv;
+            }
+            lbuf[xi] = rv;
+        }
+        __syncwarp();
+        for (int a = lane; a < nbc; a += 32) {
+            const int lo = __ldg(cd.rlo + a);
+            double s = 0.0;
+            for (int t = 0; t < rw; ++t) {
+                const int xi = lo + t;
+                if (xi >= 0 && xi < nb) s += __ldg(cd.rval + a * rw + t) * lbuf[xi];
+            }
+            cd.t1[(size_t)line * nbc + a] = s;
+        }
+        __syncwarp();
+    }
+}
+
+// rc[(c nbc + b) nbc + a] = sum_{z, y} R[c][z] R[b][y] t1[z nb + y][a], one warp per coarse DOF
+__device__ __forceinline__ void tl_restrict(const CoarseDev& cd) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int nb = cd.nb, nbc = cd.nbc, rw = cd.rw;
+    for (int q = gw; q < cd.ncg; q += nw) {
+        const int a = q % nbc, b = (q / nbc) % nbc, c = q / (nbc * nbc);
+        const int ylo = __ldg(cd.rlo + b), zlo = __ldg(cd.rlo + c);
+        double s = 0.0;
+        for (int t = lane; t < rw * rw; t += 32) {
+            const int tz = t / rw, ty = t - tz * rw;
+            const int z = zlo + tz, y = ylo + ty;
+            if (z >= 0 && z < nb && y >= 0 && y < nb)
+                s += __ldg(cd.rval + c * rw + tz) * __ldg(cd.rval + b * rw + ty) *
+                     __ldcg(cd.t1 + ((size_t)z * nb + y) * nbc + a);
+        }
+        s = warp_sum(s);
+        if (lane == 0) cd.rc[q] = s;
+    }
+}
+
+// yc = Ac^-1 rc: rc staged in shared memory, one warp per row
+__device__ __forceinline__ void tl_coarse_solve(const CoarseDev& cd, double* srb) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int ncg = cd.ncg;
+    for (int i = threadIdx.x; i < ncg; i += blockDim.x) srb[i] = __ldcg(cd.rc + i);
+    __syncthreads();
+    for (int row = gw; row < ncg; row += nw) {
+        const double* m = cd.minv + (size_t)row * ncg;
+        double s = 0.0;
+        for (int col = lane; col < ncg; col += 32) s += __ldg(m + col) * srb[col];
+        s = warp_sum(s);
+        if (lane == 0) cd.yc[row] = s;
+    }
+    __syncthreads();
+}
+
+// One patch of the two-level step, by one warp: r' = r - A zc on the patch,
+// z = zc + B_P r' (exact block, or Jacobi), and this lane's shares of r.z and
+// r_old.z.
+__device__ __forceinline__ void tl_patch_step(const LearnedArgs& L, const CoarseDev& cd, const PcgBufs& B, int k,
+                                              double& rz, double& roz) {
+    const int l = threadIdx.x & 31;
+    const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
+    const double r0 = j0 >= 0 ? __ldcg(B.r + j0) : 0.0, r1 = j1 >= 0 ? __ldcg(B.r + j1) : 0.0;
+    const double q0 = j0 >= 0 ? r0 - __ldcg(cd.azc + j0) : 0.0, q1 = j1 >= 0 ? r1 - __ldcg(cd.azc + j1) : 0.0;
+    const int slot = L.pm.slot ? __ldg(L.pm.slot + k) : -1;
+    double w0, w1;
+    if (slot >= 0 && L.pm.binv) {  // exact block solve, columns read coalesced (the inverse is symmetric)
+        const double* Bk = L.pm.binv + (size_t)slot * 4096;
+        w0 = 0.0;
+        w1 = 0.0;
+#pragma unroll 8
+        for (int q = 0; q < 64; ++q) {
+            const double rq = __shfl_sync(0xffffffffu, q < 32 ? q0 : q1, q & 31);
+            w0 += __ldg(Bk + q * 64 + l) * rq;
+            w1 += __ldg(Bk + q * 64 + l + 32) * rq;
+        }
+    } else {
+        w0 = j0 >= 0 ? __ldg(B.dinv + j0) * q0 : 0.0;
+        w1 = j1 >= 0 ? __ldg(B.dinv + j1) * q1 : 0.0;
+    }
+    if (j0 >= 0) {
+        const double z0 = __ldcg(cd.zc + j0) + w0;
+        L.z[j0] = z0;
+        rz += r0 * z0;
+        roz += __ldcg(L.rold + j0) * z0;
+    }
+    if (j1 >= 0) {
+        const double z1 = __ldcg(cd.zc + j1) + w1;
+        L.z[j1] = z1;
+        rz += r1 * z1;
+        roz += __ldcg(L.rold + j1) * z1;
+    }
+}
+
+// z = M(r) from t1 (already formed by tl_update_lines): restriction, coarse
+// solve, prolongation + A zc, patch step; leaves this block's r.z and r_old.z
+// partials in part slots 3 and 5 (the caller syncs the grid before reading
+// them).  False if a grid barrier gave up.
+template <class Op>
+__device__ __forceinline__ bool tl_precond(const Op& op, const CoarseDev& cd, const LearnedArgs& L, const PcgBufs& B,
+                                           const GridSync& gs, double* sm, double* sh) {
+    const int nb = gridDim.x;
+    const int warp = threadIdx.x >> 5;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
+    tl_restrict(cd);
+    if (!grid_sync(gs)) return false;
+    tl_coarse_solve(cd, sm);
+    if (!grid_sync(gs)) return false;
+    for (int i = threadIdx.x; i < cd.ncg; i += blockDim.x) sm[i] = __ldcg(cd.yc + i);
+    __syncthreads();
+    op.phase0_from(ProlongFn{cd, op.td.ext.full_of_red, sm}, cd.zc);
+    if (!grid_sync(gs)) return false;
+    (void)op.apply_tail(cd.zc, cd.azc, gs, sm);
+    if (grid_error(gs) || !grid_sync(gs)) return false;
+    double rz = 0.0, roz = 0.0;
+    for (int q = gw; q < L.pm.n_patch; q += nw) tl_patch_step(L, cd, B, q, rz, roz);
+    rz = block_sum(rz, sh);
+    roz = block_sum(roz, sh);
+    if (threadIdx.x == 0) {
+        B.part[3 * nb + blockIdx.x] = rz;
+        B.part[5 * nb + blockIdx.x] = roz;
+    }
+    return true;
+}
+
+// Two-level flexible PCG (Polak-Ribiere beta).  Per iteration:
+//   apply:  p = z + beta p_old fused into phase 0, A p, p.A p   (operator barriers)
+//   barrier, alpha
+//   lines:  x += alpha p, r -= alpha A p, r.r, x-contraction of r
+//   barrier, convergence test on ||r|| / ||b||
+//   z = M(r) (tl_precond), barrier, beta = (r.z - r_old.z) / r.z_old
+template <class Op>
+__global__ void __launch_bounds__(CUTCELL_BLOCK, 2) tlpcg_kernel(Op op, SolveArgs a, LearnedArgs L, CoarseDev cd) {
+    static_assert(Op::kFusedP, "the two-level PCG forms p inside the operator's first phase");
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double sh[CUTCELL_WARPS + 1];
+    const PcgBufs& B = a.B;
+    const int n = B.n, nb = gridDim.x;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    double* lbuf = sm + (size_t)(threadIdx.x >> 5) * cd.nb;
+    double* part = B.part;
+    const GridSync& gs = a.gs;
+    double bb = 0.0;
+    for (int i = gtid; i < n; i += gstride) {
+        a.x[i] = 0.0;
+        B.r[i] = a.b[i];
+        bb += a.b[i] * a.b[i];
+    }
+    bb = block_sum(bb, sh);
+    if (threadIdx.x == 0) part[1 * nb + blockIdx.x] = bb;
+    int status = CUTCELL_E_NOCONV, k = 0;
+    double rel = 1.0;
+    if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
+    double bnorm = sqrt(grid_reduce(part + 1 * nb, nb, sh));
+    if (bnorm == 0.0) bnorm = 1.0;
+    // z = M(b), p = z, rz
+    double rr = 0.0;
+    double rz = 0.0;
+    if (status != CUTCELL_E_BARRIER) {
+        tl_update_lines(cd, op.td.ext, B, L.rold, 0.0, B.p, a.x, lbuf, rr);
+        if (!grid_sync(gs) || !tl_precond(op, cd, L, B, gs, sm, sh) || !grid_sync(gs)) status = CUTCELL_E_BARRIER;
+    }
+    if (status != CUTCELL_E_BARRIER) {
+        rz = grid_reduce(part + 3 * nb, nb, sh);
+        for (int i = gtid; i < n; i += gstride) B.p[i] = __ldcg(L.z + i);
+        if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
+    }
+    double* P[2] = {B.p, B.p2};
+    double beta = 0.0;
+    for (k = 1; k <= a.maxiter && status != CUTCELL_E_BARRIER; ++k) {
+        double* pk = P[(k - 1) & 1];
+        double pap = (k > 1) ? op.apply_next(P[k & 1], pk, L.z, L.ones, beta, B.Ap, gs, sm) : op.apply(pk, B.Ap, gs, sm);
+        if (grid_error(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        pap = block_sum(pap, sh);
+        if (threadIdx.x == 0) part[2 * nb + blockIdx.x] = pap;
+        if (!grid_sync(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        pap = grid_reduce(part + 2 * nb, nb, sh);
+        if (!(pap > 0.0) || !isfinite(pap)) {
+            status = CUTCELL_E_BREAKDOWN;
+            break;
+        }
+        const double alpha = rz / pap;
+        rr = 0.0;
+        tl_update_lines(cd, op.td.ext, B, L.rold, alpha, pk, a.x, lbuf, rr);
+        rr = block_sum(rr, sh);
+        if (threadIdx.x == 0) part[4 * nb + blockIdx.x] = rr;
+        if (!grid_sync(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        rel = sqrt(grid_reduce(part + 4 * nb, nb, sh)) / bnorm;
+        if (!isfinite(rel)) {
+            status = CUTCELL_E_NAN;
+            break;
+        }
+        if (rel <= a.tol) {
+            status = CUTCELL_OK;
+            break;
+        }
+        if (!tl_precond(op, cd, L, B, gs, sm, sh) || !grid_sync(gs)) {
+            status = CUTCELL_E_BARRIER;
+            break;
+        }
+        const double rzn = grid_reduce(part + 3 * nb, nb, sh);
+        const double roz_n = grid_reduce(part + 5 * nb, nb, sh);
+        beta = (rzn - roz_n) / rz;
+        rz = rzn;
+    }
+    const int iters = k > a.maxiter ? a.maxiter : k;
+    double true_rel = -1.0;
+    if (status != CUTCELL_E_BARRIER && !grid_error(gs))
+        true_rel = true_residual(op, B, a.b, a.x, bnorm, gs, sm, sh, nullptr);
+    if (grid_error(gs)) status = CUTCELL_E_BARRIER;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.res->status = status;
+        a.res->iterations = iters;
+        a.res->outer = 1;
+        a.res->rel = rel;
+        a.res->true_rel = true_rel;
+    }
+}

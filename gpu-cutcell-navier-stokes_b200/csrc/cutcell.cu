@@ -11,6 +11,7 @@
 
 #include "pcg.cuh"
 #include "learned.cuh"
+#include "coarse.cuh"
 #include "fastdiag.cuh"
 #include "kron.cuh"
 #include "dgemm.cuh"
@@ -191,6 +192,10 @@ struct cutcell_ctx {
     int* pslot_all = nullptr;  // identity patch -> block map of cutcell_pcg_set_block_inverses
     double* zl = nullptr;
     double* rold = nullptr;
+    // two-level preconditioner: coarse-grid tables (caller-owned) and work arrays
+    bool has_coarse = false;
+    CoarseDev coarse = {};
+    double* cwork = nullptr;  // t1 | rc | yc | zc | azc
     // reduced-precision forms: residual-replacement factor and cap
     double inner_tol = 0.1;
     int inner_maxiter = 0;
@@ -310,6 +315,28 @@ static int run_fcg(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, c
     return launch_coop(kern, *blocks, smem, s, op, a, L, op_al);
 }
 
+// Two-level patch PCG: shared memory of the operator, or the staged coarse
+// vector and the per-warp x-lines if larger.
+template <class Op>
+static int run_tl(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, cudaStream_t s, int* blocks) {
+    size_t smem = op_smem;
+    const size_t need = std::max((size_t)c->coarse.ncg, (size_t)CUTCELL_WARPS * c->coarse.nb) * sizeof(double);
+    if (need > smem) smem = need;
+    smem = (smem + 15) & ~(size_t)15;
+    LearnedArgs L;
+    memset(&L, 0, sizeof(L));
+    L.pm = c->pmap;
+    L.z = c->zl;
+    L.rold = c->rold;
+    L.ones = c->ones;
+    auto kern = tlpcg_kernel<Op>;
+    int st = ensure_part(c, kern, smem, blocks);
+    if (st) return st;
+    a.gs = make_gs(c, *blocks);
+    a.B = make_bufs(c);
+    return launch_coop(kern, *blocks, smem, s, op, a, L, c->coarse);
+}
+
 template <class Op>
 static int run_apply(cutcell_ctx* c, const Op& op, size_t smem, const double* x, double* y, cudaStream_t s) {
     auto kern = apply_kernel<Op>;
@@ -336,6 +363,7 @@ static int tiles_run(cutcell_ctx* c, int mode, int precision, SolveArgs* a, cons
     const size_t sm = TileOp<double, P1>::smem_bytes();
     if (mode == 2) return run_fcg(c, o64, sm, *a, s, blocks, 1);
     if (mode == 3) return run_fcg(c, o64, sm, *a, s, blocks, 2);
+    if (mode == 4) return run_tl(c, o64, sm, *a, s, blocks);
     if (mode == 1) {
         if (precision == CUTCELL_FP64) return run_apply(c, o64, sm, x, y, s);
         if (precision == CUTCELL_FP32_IR) return run_apply(c, o32, sm, x, y, s);
@@ -838,12 +866,18 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
                       int32_t precond, CutcellReport* report, void* stream) {
     if (!c || !b || !x || maxiter < 0 || !(tol >= 0.0)) return CUTCELL_E_ARG;
     if (precision < CUTCELL_FP64 || precision > CUTCELL_BF16_IR) return CUTCELL_E_ARG;
-    if (precond < CUTCELL_PRECOND_NONE || precond > CUTCELL_PRECOND_BLOCK) return CUTCELL_E_ARG;
+    if (precond < CUTCELL_PRECOND_NONE || precond > CUTCELL_PRECOND_TWOLEVEL) return CUTCELL_E_ARG;
     if (precond == CUTCELL_PRECOND_JACOBI_LEARNED && (!c->mlp || precision != CUTCELL_FP64 || c->kind != KIND_TILES))
         return CUTCELL_E_ARG;
     if (precond == CUTCELL_PRECOND_BLOCK &&
         (!c->pmap.binv || !c->pmap.slot || !c->zl || precision != CUTCELL_FP64 || c->kind != KIND_TILES)) {
         g_last_error = "CUTCELL_PRECOND_BLOCK needs patch blocks (cutcell_pcg_set_patch_blocks), FP64, a tile context";
+        return CUTCELL_E_ARG;
+    }
+    if (precond == CUTCELL_PRECOND_TWOLEVEL &&
+        (!c->has_coarse || !c->pmap.red || !c->zl || precision != CUTCELL_FP64 || c->kind != KIND_TILES)) {
+        g_last_error = "CUTCELL_PRECOND_TWOLEVEL needs a coarse level (cutcell_pcg_set_coarse), a patch layout "
+                       "(cutcell_pcg_set_patch_blocks), FP64, a tile context";
         return CUTCELL_E_ARG;
     }
     if (c->kind == KIND_KRON && precision != CUTCELL_FP64) {
@@ -882,6 +916,8 @@ int cutcell_pcg_solve(cutcell_ctx* c, const double* b, double* x, double tol, in
         st = tiles_dispatch(c, 2, precision, &a, nullptr, nullptr, s, &blocks);
     } else if (precond == CUTCELL_PRECOND_BLOCK) {
         st = tiles_dispatch(c, 3, precision, &a, nullptr, nullptr, s, &blocks);
+    } else if (precond == CUTCELL_PRECOND_TWOLEVEL) {
+        st = tiles_dispatch(c, 4, precision, &a, nullptr, nullptr, s, &blocks);
     } else {
         st = tiles_dispatch(c, 0, precision, &a, nullptr, nullptr, s, &blocks);
     }
@@ -945,7 +981,7 @@ int cutcell_ext_scatter(cutcell_ctx* c, const double* y_full, double* y_red, voi
 int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);  // cudaFree below waits for the work that may still use the buffers
-    void* bufs[] = {c->pslot_all, c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->cwork, c->pslot_all, c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
                     c->p,     c->p2,    c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -1098,6 +1134,51 @@ int cutcell_pcg_set_patch_blocks(cutcell_ctx* c, const int32_t* patch_red, int32
         CK(cudaMalloc(&c->zl, (size_t)c->n * sizeof(double)));
         CK(cudaMalloc(&c->rold, (size_t)c->n * sizeof(double)));
     }
+    return CUTCELL_OK;
+}
+
+int cutcell_pcg_set_coarse(cutcell_ctx* c, const CutcellCoarseDesc* d) {
+    if (!c || c->kind != KIND_TILES) return CUTCELL_E_ARG;
+    if (!d) {
+        c->has_coarse = false;
+        return CUTCELL_OK;
+    }
+    const int nb = c->td.n + c->td.p;
+    if (d->nb != nb || d->nbc < 1 || d->nbc > nb || d->pw < 1 || d->pw > d->nbc || d->rw < 1 || d->rw > nb ||
+        !d->plo || !d->pval || !d->rlo || !d->rval || !d->minv) {
+        g_last_error = "coarse level: fine DOFs per axis must be n + p, band widths within the grids, all tables set";
+        return CUTCELL_E_ARG;
+    }
+    const long long ncg = (long long)d->nbc * d->nbc * d->nbc;
+    if (ncg > 16384) {
+        g_last_error = "coarse level: at most 16384 coarse DOFs (the dense inverse is read every iteration)";
+        return CUTCELL_E_SHAPE;
+    }
+    if (c->cwork) cudaFree(c->cwork);
+    c->cwork = nullptr;
+    const size_t nt1 = (size_t)nb * nb * d->nbc;
+    CK(cudaMalloc(&c->cwork, (nt1 + 2 * (size_t)ncg + 2 * (size_t)c->n) * sizeof(double)));
+    CoarseDev& cd = c->coarse;
+    cd.nb = nb;
+    cd.nbc = d->nbc;
+    cd.ncg = (int)ncg;
+    cd.pw = d->pw;
+    cd.rw = d->rw;
+    cd.plo = d->plo;
+    cd.pval = d->pval;
+    cd.rlo = d->rlo;
+    cd.rval = d->rval;
+    cd.minv = d->minv;
+    cd.t1 = c->cwork;
+    cd.rc = cd.t1 + nt1;
+    cd.yc = cd.rc + ncg;
+    cd.zc = cd.yc + ncg;
+    cd.azc = cd.zc + c->n;
+    if (!c->zl) {
+        CK(cudaMalloc(&c->zl, (size_t)c->n * sizeof(double)));
+        CK(cudaMalloc(&c->rold, (size_t)c->n * sizeof(double)));
+    }
+    c->has_coarse = true;
     return CUTCELL_OK;
 }
 

@@ -32,6 +32,7 @@ PRECOND_NONE = 0
 PRECOND_JACOBI = 1
 PRECOND_JACOBI_LEARNED = 2
 PRECOND_BLOCK = 3
+PRECOND_TWOLEVEL = 4
 MLP_NPARAM = 16576
 MLP_IN, MLP_H, MLP_OUT = 128, 64, 64
 
@@ -109,6 +110,12 @@ class CutcellHillDesc(C.Structure):
     ]
 
 
+class CutcellCoarseDesc(C.Structure):
+    _fields_ = [(f, C.c_int32) for f in ("nb", "nbc", "pw", "rw")] + [
+        (f, _P) for f in ("plo", "pval", "rlo", "rval", "minv")
+    ]
+
+
 class CutcellBatchConfig(C.Structure):
     _fields_ = [
         ("cluster", C.c_int32),
@@ -141,6 +148,7 @@ SIGNATURES = {
     "cutcell_pcg_set_learned": (C.c_int, [_P, _P, _P, _P, C.c_int32]),
     "cutcell_pcg_set_block_inverses": (C.c_int, [_P, _P]),
     "cutcell_pcg_set_patch_blocks": (C.c_int, [_P, _P, C.c_int32, _P, _P]),
+    "cutcell_pcg_set_coarse": (C.c_int, [_P, _P]),
     "cutcell_fastdiag_create": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "cutcell_fastdiag_solve": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
     "cutcell_fastdiag_destroy": (C.c_int, [_P]),

@@ -27,7 +27,7 @@ import scipy.sparse as sp
 from . import _lib
 
 Backend = Literal["b200", "gpu", "auto"]
-Preconditioner = Literal["none", "jacobi", "jacobi+learned", "block"]
+Preconditioner = Literal["none", "jacobi", "jacobi+learned", "block", "twolevel"]
 Precision = Literal["fp64", "fp32-ir", "bf16-ir"]
 
 
@@ -227,7 +227,7 @@ def solve_spd(
             f"backend {backend!r} is not provided here: this package only ships the B200 solver "
             "(use the reference's SciPy path for backend='cpu')"
         )
-    if preconditioner in ("jacobi+learned", "block"):
+    if preconditioner in ("jacobi+learned", "block", "twolevel"):
         from .learned import solve_learned
 
         return solve_learned(A, b, tol=tol, maxiter=maxiter, precision=precision, preconditioner=preconditioner, **kw)

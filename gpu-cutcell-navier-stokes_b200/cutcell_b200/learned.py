@@ -440,11 +440,13 @@ def attach(op: CutCellOperator, mlp: PatchMLP | None) -> None:
 
 def solve_learned(A, b, *, tol=1e-8, maxiter=5000, precision="fp64", mlp: PatchMLP | None = None,
                   preconditioner: str = "jacobi+learned", **_):
-    """``solve_spd(..., preconditioner="jacobi+learned" | "block")`` on a
-    ``CutCellOperator``: flexible PCG with exact solves on the non-canonical
-    patches and the attached (or given) network on the canonical ones
-    ("jacobi+learned"), or exact solves on every patch ("block", the
-    block-Jacobi ceiling of patch-local corrections)."""
+    """``solve_spd(..., preconditioner="jacobi+learned" | "block" |
+    "twolevel")`` on a ``CutCellOperator``: flexible PCG with exact solves on
+    the non-canonical patches and the attached (or given) network on the
+    canonical ones ("jacobi+learned"), exact solves on every patch ("block",
+    the block-Jacobi ceiling of patch-local corrections), or the Galerkin
+    coarse-grid correction followed by the exact patch solves ("twolevel",
+    ``coarse.attach_coarse``)."""
     from time import perf_counter
 
     import torch
@@ -452,7 +454,7 @@ def solve_learned(A, b, *, tol=1e-8, maxiter=5000, precision="fp64", mlp: PatchM
     from .fast_solver_backends import _report_from
 
     if not isinstance(A, CutCellOperator):
-        raise ValueError("the patch preconditioners need the matrix-free CutCellOperator")
+        raise ValueError("the patch and two-level preconditioners need the matrix-free CutCellOperator")
     if precision != "fp64":
         raise ValueError("the patch preconditioners run in FP64 flexible PCG")
     if preconditioner == "jacobi+learned":
@@ -461,6 +463,12 @@ def solve_learned(A, b, *, tol=1e-8, maxiter=5000, precision="fp64", mlp: PatchM
         attach_blocks(A, "noncanonical")
     elif preconditioner == "block":
         attach_blocks(A, "all")
+    elif preconditioner == "twolevel":
+        from .coarse import attach_coarse
+
+        attach_blocks(A, "all")
+        if getattr(A, "_coarse", None) is None:
+            attach_coarse(A)
     else:
         raise ValueError(f"unknown patch preconditioner {preconditioner!r}")
     b_np = np.asarray(b, dtype=float)

@@ -304,7 +304,7 @@ class CutCellOperator:
             x = torch.empty_like(b)
         rep = _lib.CutcellReport()
         pc = {"none": _lib.PRECOND_NONE, "jacobi": _lib.PRECOND_JACOBI, "jacobi+learned": _lib.PRECOND_JACOBI_LEARNED,
-              "block": _lib.PRECOND_BLOCK}[preconditioner]
+              "block": _lib.PRECOND_BLOCK, "twolevel": _lib.PRECOND_TWOLEVEL}[preconditioner]
         _lib.check(
             self._lib.cutcell_pcg_solve(
                 self._ctx, b.data_ptr(), x.data_ptr(), float(tol), int(maxiter), _lib.PRECISIONS[precision], pc,

@@ -41,7 +41,8 @@ enum {
     CUTCELL_PRECOND_NONE = 0,
     CUTCELL_PRECOND_JACOBI = 1,
     CUTCELL_PRECOND_JACOBI_LEARNED = 2, /* patch blocks where set, the network on the other patches */
-    CUTCELL_PRECOND_BLOCK = 3           /* patch blocks where set, Jacobi on the other patches */
+    CUTCELL_PRECOND_BLOCK = 3,          /* patch blocks where set, Jacobi on the other patches */
+    CUTCELL_PRECOND_TWOLEVEL = 4        /* Galerkin coarse-grid correction, then the patch solves */
 };
 
 typedef struct cutcell_ctx cutcell_ctx;
@@ -224,6 +225,30 @@ int cutcell_pcg_set_block_inverses(cutcell_ctx* ctx, const double* binv);
  * blocks.  All device pointers, kept by reference. */
 int cutcell_pcg_set_patch_blocks(cutcell_ctx* ctx, const int32_t* patch_red, int32_t n_patch, const int32_t* slot,
                                  const double* binv);
+
+/* Coarse level of CUTCELL_PRECOND_TWOLEVEL (no reference counterpart: a
+ * preconditioner of solve_gpu_cg's systems, code/fast_solver_backends.py:194-289).
+ * z = zc + B (r - A zc) with zc = P Ac^-1 P^T r: P the tensor product of the
+ * 1D uniform B-spline refinement R1 (nbc coarse -> nb = n + p fine functions
+ * per axis) restricted to the reduced DOFs, Ac = P^T A P, B the patch solves
+ * of cutcell_pcg_set_patch_blocks (Jacobi on patches without a block).  The
+ * 1D refinement is given twice, banded: by fine row x (coarse columns
+ * plo[x] .. plo[x] + pw - 1, values pval[x][pw]) and by coarse column a
+ * (fine rows rlo[a] .. rlo[a] + rw - 1, values rval[a][rw]); zero entries pad
+ * the bands.  minv is Ac^-1 on the full coarse grid (nbc^3 x nbc^3,
+ * row-major, coarse index (c nbc + b) nbc + a for (x, y, z) = (a, b, c)), zero
+ * rows and columns for coarse functions without fluid.  All device pointers,
+ * kept by reference; NULL desc removes the level.  At most 16384 coarse
+ * DOFs (CUTCELL_E_SHAPE). */
+typedef struct {
+    int32_t nb, nbc, pw, rw;
+    const int32_t* plo;
+    const double* pval;
+    const int32_t* rlo;
+    const double* rval;
+    const double* minv;
+} CutcellCoarseDesc;
+int cutcell_pcg_set_coarse(cutcell_ctx* ctx, const CutcellCoarseDesc* desc);
 
 /* ---- periodic-hill fast diagonalisation (FastDiagHill, cpp/include/cut/hill_fastdiag.h:20-80) ----
  * create: the reduced 2D forms M2, Qx2, Qy2 (nr x nr, row-major), the z

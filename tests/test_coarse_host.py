@@ -1,0 +1,67 @@
+"""Host tables of the two-level preconditioner (no GPU): the 1D B-spline
+refinement is exact, its bands reproduce it, the coarsening rule, and the
+prolongation P selects the kept DOFs' rows of R1 (x) R1 (x) R1."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cutcell_b200.bspline import global_values, make_basis
+from cutcell_b200.coarse import _bands, coarse_factor, prolongation, refinement_1d
+
+
+@pytest.mark.parametrize("n,p,c", [(8, 3, 2), (32, 3, 4), (12, 2, 2), (16, 4, 4), (24, 3, 4)])
+def test_refinement_is_exact(n, p, c):
+    R = refinement_1d(n, p, c)
+    fb, cb = make_basis(n, p), make_basis(n // c, p)
+    x = np.random.default_rng(1).uniform(0.0, 1.0, 400)
+    np.testing.assert_allclose(global_values(fb, x) @ R, global_values(cb, x), atol=1e-13)
+    # partition of unity is kept and every coarse function refines into p + 1 .. (p + 1) c + 1 - p fine ones
+    np.testing.assert_allclose(R.sum(axis=1), 1.0, atol=1e-13)
+    assert R.shape == (n + p, n // c + p)
+
+
+def test_bands_reproduce_refinement():
+    R = refinement_1d(32, 3, 4)
+    plo, pw, pval, rlo, rw, rval = _bands(R)
+    nb, nbc = R.shape
+    Rp = np.zeros_like(R)
+    Rr = np.zeros_like(R)
+    for x in range(nb):
+        assert 0 <= plo[x] and plo[x] + pw <= nbc
+        Rp[x, plo[x]:plo[x] + pw] = pval[x]
+    for a in range(nbc):
+        assert 0 <= rlo[a] and rlo[a] + rw <= nb
+        Rr[rlo[a]:rlo[a] + rw, a] = rval[a]
+    np.testing.assert_array_equal(Rp, R)
+    np.testing.assert_array_equal(Rr, R)
+    assert pw <= 4 and rw <= 13
+
+
+def test_coarse_factor_rule():
+    assert coarse_factor(8, 3) == 2
+    assert coarse_factor(16, 3) == 2
+    assert coarse_factor(24, 3) == 4
+    assert coarse_factor(32, 3) == 4
+    assert coarse_factor(64, 3) == 8
+    with pytest.raises(ValueError):
+        coarse_factor(7, 3)
+    with pytest.raises(ValueError):
+        refinement_1d(10, 3, 4)
+
+
+def test_prolongation_rows_are_kept_dofs():
+    from cutcell_b200.workloads import sphere_poisson
+
+    prob, ext = sphere_poisson(8, 3, 0.31)
+    P, R = prolongation(prob, ext, 2)
+    nb = prob.n_basis
+    full_of_red = np.asarray(ext.device_layout()["full_of_red"])
+    assert P.shape == (ext.n_red, R.shape[1] ** 3)
+    rng = np.random.default_rng(4)
+    for j in rng.choice(ext.n_red, 20, replace=False):
+        f = full_of_red[j]
+        x, y, z = f % nb, (f // nb) % nb, f // (nb * nb)
+        dense = np.einsum("c,b,a->cba", R[z], R[y], R[x]).ravel()
+        np.testing.assert_allclose(P[j].toarray().ravel(), dense, atol=1e-15)
