@@ -26,7 +26,7 @@ struct CoarseDev {
     int nb, nbc, ncg;           // fine / coarse DOFs per axis, nbc^3
     int pw, rw;                 // band widths of the prolongation rows / restriction rows
     const int* plo;             // [nb] first coarse index of fine row x (plo + pw <= nbc)
-    const double* pval;         // [nb][pw]
+    const double* pval;         // [nb][pw], pw = p + 1
     const int* rlo;             // [nbc] first fine index of coarse column a (rlo + rw <= nb)
     const double* rval;         // [nbc][rw]
     const double* minv;         // [ncg][ncg] Ac^-1, zero rows / columns for coarse DOFs without fluid
@@ -37,32 +37,43 @@ struct CoarseDev {
     double* azc;                // [n] A zc
 };
 
-// zc_j = (P yc)_j from the coarse vector in shared memory
+// zc_j = (P yc)_j from the coarse vector in shared memory.  PW = p + 1 is the
+// width of every prolongation row band (a fine B-spline lies in the support
+// of at most p + 1 coarse ones per axis); the host pads the bands to exactly
+// PW, so the loops unroll with the weights in registers.  Indices are clamped
+// into the coarse grid, so a corrupt table cannot read outside ys.
+template <int PW>
 struct ProlongFn {
     CoarseDev cd;
     const int* full_of_red;
     const double* ys;
     __device__ __forceinline__ double operator()(int j) const {
-        const int f = __ldg(full_of_red + j), nb = cd.nb, nbc = cd.nbc, pw = cd.pw;
-        const int x = f % nb, y = (f / nb) % nb, z = f / (nb * nb);
-        const int xl = __ldg(cd.plo + x), yl = __ldg(cd.plo + y), zl = __ldg(cd.plo + z);
+        const int f = __ldg(full_of_red + j), nb = cd.nb, nbc = cd.nbc;
+        const int z = f / (nb * nb), rem = f - z * nb * nb;
+        const int y = rem / nb, x = rem - y * nb;
+        const int xl = min(max(__ldg(cd.plo + x), 0), nbc - PW);
+        const int yl = min(max(__ldg(cd.plo + y), 0), nbc - PW);
+        const int zl = min(max(__ldg(cd.plo + z), 0), nbc - PW);
+        double wx[PW], wy[PW], wz[PW];
+#pragma unroll
+        for (int t = 0; t < PW; ++t) {
+            wx[t] = __ldg(cd.pval + x * PW + t);
+            wy[t] = __ldg(cd.pval + y * PW + t);
+            wz[t] = __ldg(cd.pval + z * PW + t);
+        }
         double s = 0.0;
-        for (int tz = 0; tz < pw; ++tz) {
-            const double wz = __ldg(cd.pval + z * pw + tz);
-            const int cz = zl + tz;
-            if (wz == 0.0 || cz < 0 || cz >= nbc) continue;
-            for (int ty = 0; ty < pw; ++ty) {
-                const double wy = __ldg(cd.pval + y * pw + ty);
-                const int cy = yl + ty;
-                if (wy == 0.0 || cy < 0 || cy >= nbc) continue;
-                const double* row = ys + ((size_t)cz * nbc + cy) * nbc;
+#pragma unroll
+        for (int tz = 0; tz < PW; ++tz) {
+            double sy = 0.0;
+#pragma unroll
+            for (int ty = 0; ty < PW; ++ty) {
+                const double* row = ys + ((size_t)(zl + tz) * nbc + (yl + ty)) * nbc + xl;
                 double sx = 0.0;
-                for (int tx = 0; tx < pw; ++tx) {
-                    const int cx = xl + tx;
-                    if (cx >= 0 && cx < nbc) sx += __ldg(cd.pval + x * pw + tx) * row[cx];
-                }
-                s += wz * wy * sx;
+#pragma unroll
+                for (int tx = 0; tx < PW; ++tx) sx += wx[tx] * row[tx];
+                sy += wy[ty] * sx;
             }
+            s += wz[tz] * sy;
         }
         return s;
     }
@@ -202,7 +213,7 @@ __device__ __forceinline__ bool tl_precond(const Op& op, const CoarseDev& cd, co
     if (!grid_sync(gs)) return false;
     for (int i = threadIdx.x; i < cd.ncg; i += blockDim.x) sm[i] = __ldcg(cd.yc + i);
     __syncthreads();
-    op.phase0_from(ProlongFn{cd, op.td.ext.full_of_red, sm}, cd.zc);
+    op.phase0_from(ProlongFn<Op::kDegree1>{cd, op.td.ext.full_of_red, sm}, cd.zc);
     if (!grid_sync(gs)) return false;
     (void)op.apply_tail(cd.zc, cd.azc, gs, sm);
     if (grid_error(gs) || !grid_sync(gs)) return false;

@@ -1144,9 +1144,10 @@ int cutcell_pcg_set_coarse(cutcell_ctx* c, const CutcellCoarseDesc* d) {
         return CUTCELL_OK;
     }
     const int nb = c->td.n + c->td.p;
-    if (d->nb != nb || d->nbc < 1 || d->nbc > nb || d->pw < 1 || d->pw > d->nbc || d->rw < 1 || d->rw > nb ||
+    if (d->nb != nb || d->nbc < 1 || d->nbc > nb || d->pw != c->td.p + 1 || d->pw > d->nbc || d->rw < 1 || d->rw > nb ||
         !d->plo || !d->pval || !d->rlo || !d->rval || !d->minv) {
-        g_last_error = "coarse level: fine DOFs per axis must be n + p, band widths within the grids, all tables set";
+        g_last_error = "coarse level: fine DOFs per axis must be n + p, prolongation bands p + 1 wide, restriction "
+                       "bands within the grid, all tables set";
         return CUTCELL_E_ARG;
     }
     const long long ncg = (long long)d->nbc * d->nbc * d->nbc;
@@ -1262,10 +1263,25 @@ int cutcell_fastdiag_create(int32_t nr, int32_t nz, const double* M2, const doub
     return CUTCELL_OK;
 }
 
+// Ypart[z][v][r] = sum_{k in kslice(z)} A[r][k] X_v[k] on the FP64 tensor cores
+// (dmma_tile: M = nr rows of the shared operator, N = the nvec vectors, split
+// over K by blockIdx.z); fd_sum_ksplit_kernel adds the slices in order.
+__global__ void __launch_bounds__(256) fd_dmma_kernel(int nr, const double* A, const double* X, VecSel sx,
+                                                      double* Ypart, int nvec) {
+    const int kch = (nr + gridDim.z - 1) / gridDim.z;
+    const int kb = blockIdx.z * kch, ke = min(nr, kb + kch);
+    double* Yz = Ypart + (size_t)blockIdx.z * nvec * nr;
+    dmma_tile(
+        nr, nvec, kb, ke, blockIdx.y * DG_BM, blockIdx.x * DG_BN,
+        [&](int m, int k) { return __ldg(A + (size_t)m * nr + k); },
+        [&](int v, int k) { return __ldg(X + vec_off(sx, v, nr) + k); },
+        [&](int m, int v, double val) { Yz[(size_t)v * nr + m] = val; });
+}
+
 static void fd_gemm(cudaStream_t s, int nr, const double* A, const double* X, VecSel sx, double* Y, VecSel sy,
                     int nvec, double* part) {
-    dim3 grid(ceil_div(nr, FD_TR), ceil_div(nvec, FD_TV), FD_KSPLIT);
-    fd_shared_gemm_kernel<<<grid, FD_GEMM_THREADS, 0, s>>>(nr, A, X, sx, part, nvec);
+    dim3 grid(ceil_div(nvec, DG_BN), ceil_div(nr, DG_BM), FD_KSPLIT);
+    fd_dmma_kernel<<<grid, 256, 0, s>>>(nr, A, X, sx, part, nvec);
     fd_sum_ksplit_kernel<<<ceil_div((long)nvec * nr, 256), 256, 0, s>>>(nr, nvec, FD_KSPLIT, part, Y, sy);
 }
 

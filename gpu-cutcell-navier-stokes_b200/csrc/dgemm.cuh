@@ -12,9 +12,12 @@
 //
 // Tiling: a 256-thread block computes a 64 x 64 tile of C; its 8 warps are
 // arranged 2 (M) x 4 (N), each owning 32 x 16 = 4 x 2 mma tiles of 8 x 8.  K is
-// staged in chunks of 16 through shared memory, transposed so that both
-// fragments read k-major rows (lane 4g + t reads row k0 + t, column g); the
-// next chunk is loaded into registers while the current one is multiplied.
+// staged in chunks of 16 through shared memory as it lies in global memory
+// (row m, k contiguous), rows padded to 20 doubles: a half-warp's staging
+// store (16 consecutive k of one row) and a half-warp's fragment read (lane
+// 4g + t reads row g, column k0 + t, g < 4) then fall in 16 distinct 8-byte
+// bank pairs.  The next chunk is loaded into registers while the current one
+// is multiplied.
 #pragma once
 
 #include "common.cuh"
@@ -22,7 +25,7 @@
 #define DG_BM 64
 #define DG_BN 64
 #define DG_BK 16
-#define DG_PAD 4
+#define DG_KS (DG_BK + 4)  // padded row of a staged chunk
 
 struct DgemmArgs {
     int M, N, K;
@@ -43,15 +46,14 @@ __device__ __forceinline__ void dg_mma(double& d0, double& d1, double a, double 
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(256) dgemm_nt_kernel(DgemmArgs g) {
-    __shared__ double As[DG_BK][DG_BM + DG_PAD];
-    __shared__ double Bs[DG_BK][DG_BN + DG_PAD];
-    const int b = blockIdx.z;
-    const double* A = g.A + (size_t)b * g.sA;
-    const double* B = g.B + (size_t)b * g.sB;
-    const double* S = g.s ? g.s + (size_t)b * g.sS : nullptr;
-    double* C = g.C + (size_t)b * g.sC;
-    const int m0 = blockIdx.y * DG_BM, n0 = blockIdx.x * DG_BN;
+// One 64 x 64 tile of C = A B^T over k in [kb, ke) by a 256-thread block:
+// a(m, k) and b(n, k) return the operand entries (callers return 0 outside
+// their ranges), store(m, n, v) receives every entry of the tile inside M x N.
+template <class AL, class BL, class CS>
+__device__ __forceinline__ void dmma_tile(int M, int N, int kb, int ke, int m0, int n0, const AL& a, const BL& b,
+                                          const CS& store) {
+    __shared__ double As[DG_BM][DG_KS];
+    __shared__ double Bs[DG_BN][DG_KS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gq = lane >> 2, t4 = lane & 3;
     const int wm = (warp >> 2) * 32, wn = (warp & 3) * 16;
@@ -61,7 +63,7 @@ __global__ void __launch_bounds__(256) dgemm_nt_kernel(DgemmArgs g) {
 #pragma unroll
         for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     // staging: 64 x 16 entries of each operand, 4 per thread; thread e loads
-    // row e / 16, column e % 16 (consecutive threads, consecutive columns)
+    // row e / 16, column e % 16 (consecutive threads, consecutive k)
     double ra[4], rb[4];
     auto load = [&](int k0) {
 #pragma unroll
@@ -69,37 +71,30 @@ __global__ void __launch_bounds__(256) dgemm_nt_kernel(DgemmArgs g) {
             const int e = threadIdx.x + 256 * u;
             const int r = e >> 4, c = e & 15;
             const int k = k0 + c;
-            double av = 0.0, bv = 0.0;
-            if (k < g.K) {
-                if (m0 + r < g.M) {
-                    av = __ldg(A + (size_t)(m0 + r) * g.lda + k);
-                    if (S) av *= __ldg(S + k);
-                }
-                if (n0 + r < g.N) bv = __ldg(B + (size_t)(n0 + r) * g.ldb + k);
-            }
-            ra[u] = av;
-            rb[u] = bv;
+            const bool kin = k < ke;
+            ra[u] = (kin && m0 + r < M) ? a(m0 + r, k) : 0.0;
+            rb[u] = (kin && n0 + r < N) ? b(n0 + r, k) : 0.0;
         }
     };
-    load(0);
-    for (int k0 = 0; k0 < g.K; k0 += DG_BK) {
+    load(kb);
+    for (int k0 = kb; k0 < ke; k0 += DG_BK) {
         __syncthreads();  // the previous chunk's fragments have been read
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int e = threadIdx.x + 256 * u;
             const int r = e >> 4, c = e & 15;
-            As[c][r] = ra[u];
-            Bs[c][r] = rb[u];
+            As[r][c] = ra[u];
+            Bs[r][c] = rb[u];
         }
         __syncthreads();
-        if (k0 + DG_BK < g.K) load(k0 + DG_BK);  // next chunk in flight during the products
+        if (k0 + DG_BK < ke) load(k0 + DG_BK);  // next chunk in flight during the products
 #pragma unroll
         for (int ks = 0; ks < DG_BK; ks += 4) {
             double af[4], bf[2];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) af[i] = As[ks + t4][wm + 8 * i + gq];
+            for (int i = 0; i < 4; ++i) af[i] = As[wm + 8 * i + gq][ks + t4];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) bf[j] = Bs[ks + t4][wn + 8 * j + gq];
+            for (int j = 0; j < 2; ++j) bf[j] = Bs[wn + 8 * j + gq][ks + t4];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -110,16 +105,32 @@ __global__ void __launch_bounds__(256) dgemm_nt_kernel(DgemmArgs g) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int m = m0 + wm + 8 * i + gq;
-        if (m >= g.M) continue;
+        if (m >= M) continue;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int n = n0 + wn + 8 * j + 2 * t4 + h;
-                if (n >= g.N) continue;
-                double* cp = C + (size_t)m * g.ldc + n;
-                *cp = (g.beta != 0.0 ? g.beta * *cp : 0.0) + acc[i][j][h];
+                if (n < N) store(m, n, acc[i][j][h]);
             }
         }
     }
+}
+
+static __global__ void __launch_bounds__(256) dgemm_nt_kernel(DgemmArgs g) {
+    const int bz = blockIdx.z;
+    const double* A = g.A + (size_t)bz * g.sA;
+    const double* B = g.B + (size_t)bz * g.sB;
+    const double* S = g.s ? g.s + (size_t)bz * g.sS : nullptr;
+    double* C = g.C + (size_t)bz * g.sC;
+    const long long lda = g.lda, ldb = g.ldb, ldc = g.ldc;
+    const double beta = g.beta;
+    dmma_tile(
+        g.M, g.N, 0, g.K, blockIdx.y * DG_BM, blockIdx.x * DG_BN,
+        [&](int m, int k) { return S ? __ldg(A + (size_t)m * lda + k) * __ldg(S + k) : __ldg(A + (size_t)m * lda + k); },
+        [&](int n, int k) { return __ldg(B + (size_t)n * ldb + k); },
+        [&](int m, int n, double v) {
+            double* cp = C + (size_t)m * ldc + n;
+            *cp = (beta != 0.0 ? beta * *cp : 0.0) + v;
+        });
 }

@@ -85,68 +85,11 @@ __device__ __forceinline__ size_t vec_off(const VecSel& s, int v, int nr) {
     return ((size_t)k * s.slots + s.first + q) * nr;
 }
 
-#define FD_TR 64
-#define FD_TV 64
-#define FD_TK 16
-#define FD_GEMM_THREADS 256
+// Shared-operator products Y_v = A X_v of the solve split the inner dimension
+// into FD_KSPLIT slices (fd_dmma_kernel, the FP64 tensor-core tile of
+// dgemm.cuh); slice z of vector v sits at Ypart + (z * nvec + v) * nr and
+// fd_sum_ksplit_kernel adds the slices in order (deterministic, no atomics).
 #define FD_KSPLIT 4
-// 256 threads as 16 x 16, each owning a 4-row x 4-vector register tile of the
-// 64 x 64 block tile.  blockIdx.z takes one of FD_KSPLIT slices of the inner
-// dimension and writes its partial product to slice z of Ypart (vector v of
-// slice z at Ypart + (z * nvec + v) * nr); fd_sum_ksplit_kernel adds the
-// slices in order (deterministic, no atomics).
-__global__ void __launch_bounds__(FD_GEMM_THREADS) fd_shared_gemm_kernel(int nr, const double* A, const double* X,
-                                                                        VecSel sx, double* Ypart, int nvec) {
-    __shared__ double As[FD_TK][FD_TR + 2];
-    __shared__ double Xs[FD_TK][FD_TV + 2];
-    const int r0 = blockIdx.x * FD_TR, v0 = blockIdx.y * FD_TV;
-    const int kchunk = (nr + gridDim.z - 1) / gridDim.z;
-    const int kb = blockIdx.z * kchunk, ke = min(nr, kb + kchunk);
-    const int tr = threadIdx.x % 16, tv = threadIdx.x / 16;
-    double acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    for (int j0 = kb; j0 < ke; j0 += FD_TK) {
-        for (int e = threadIdx.x; e < FD_TR * FD_TK; e += blockDim.x) {
-            const int rr = e / FD_TK, jj = e % FD_TK;
-            const int r = r0 + rr, j = j0 + jj;
-            As[jj][rr] = (r < nr && j < ke) ? A[(size_t)r * nr + j] : 0.0;
-        }
-        for (int e = threadIdx.x; e < FD_TV * FD_TK; e += blockDim.x) {
-            const int vv = e / FD_TK, jj = e % FD_TK;
-            const int v = v0 + vv, j = j0 + jj;
-            Xs[jj][vv] = (v < nvec && j < ke) ? X[vec_off(sx, v, nr) + j] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int jj = 0; jj < FD_TK; ++jj) {
-            double a[4], x[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                a[q] = As[jj][tr + 16 * q];
-                x[q] = Xs[jj][tv + 16 * q];
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int w = 0; w < 4; ++w) acc[q][w] += a[q] * x[w];
-        }
-        __syncthreads();
-    }
-    double* Yz = Ypart + (size_t)blockIdx.z * nvec * nr;
-#pragma unroll
-    for (int w = 0; w < 4; ++w) {
-        const int v = v0 + tv + 16 * w;
-        if (v >= nvec) continue;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int r = r0 + tr + 16 * q;
-            if (r < nr) Yz[(size_t)v * nr + r] = acc[q][w];
-        }
-    }
-}
 
 // Y[sel(v)] = sum_z Ypart[z][v]  (slices added in order)
 __global__ void fd_sum_ksplit_kernel(int nr, int nvec, int ks, const double* Ypart, double* Y, VecSel sy) {

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "dgemm.cuh"
 
 void cutcell_internal_set_error(const std::string& what);
 
@@ -265,62 +266,22 @@ __global__ void hill_gather_kernel(HillAdvDev d, const double* part, double* T) 
             const double rj = __shfl_sync(0xffffffffu, r[c], jz);
             if (lane < nz) t = fma(d.Mzinv[lane * nz + jz], rj, t);
         }
-        if (lane < nz) T[(size_t)m * 3 * nz + c * nz + lane] = t;
+        if (lane < nz) T[(size_t)(c * nz + lane) * d.nr + m] = t;
     }
 }
 
-// C_part[z] = A[:, kslice(z)] B[kslice(z), :] for row-major A (n x n) and
-// B (n x ncol); 64 x 64 tile, 256 threads with 4 x 4 register tiles.
-#define HG_T 64
-#define HG_K 16
-__global__ void __launch_bounds__(256) hill_gemm_kernel(int n, int ncol, const double* A, const double* B, double* Cp) {
-    __shared__ double As[HG_K][HG_T + 2];
-    __shared__ double Bs[HG_K][HG_T + 2];
-    const int r0 = blockIdx.x * HG_T, c0 = blockIdx.y * HG_T;
+// C_part[z] = A[:, kslice(z)] B[kslice(z), :] for row-major A (n x n) and B
+// given transposed (BT: ncol x n, row col = column col of B), on the FP64
+// tensor cores (dmma_tile, 64 x 64 tiles, split over K by blockIdx.z).
+__global__ void __launch_bounds__(256) hill_gemm_kernel(int n, int ncol, const double* A, const double* BT, double* Cp) {
     const int kch = (n + gridDim.z - 1) / gridDim.z;
     const int kb = blockIdx.z * kch, ke = min(n, kb + kch);
-    const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
-    double acc[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-    for (int j0 = kb; j0 < ke; j0 += HG_K) {
-        for (int e = threadIdx.x; e < HG_T * HG_K; e += 256) {
-            const int rr = e / HG_K, jj = e % HG_K;
-            const int r = r0 + rr, j = j0 + jj;
-            As[jj][rr] = (r < n && j < ke) ? A[(size_t)r * n + j] : 0.0;
-            const int jb = e / HG_T, cc = e % HG_T;
-            const int jj2 = j0 + jb, col = c0 + cc;
-            Bs[jb][cc] = (jj2 < ke && col < ncol) ? B[(size_t)jj2 * ncol + col] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int jj = 0; jj < HG_K; ++jj) {
-            double a[4], b[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                a[q] = As[jj][tr + 16 * q];
-                b[q] = Bs[jj][tc + 16 * q];
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int v = 0; v < 4; ++v) acc[q][v] = fma(a[q], b[v], acc[q][v]);
-        }
-        __syncthreads();
-    }
     double* Cz = Cp + (size_t)blockIdx.z * n * ncol;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int r = r0 + tr + 16 * q;
-        if (r >= n) continue;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int col = c0 + tc + 16 * v;
-            if (col < ncol) Cz[(size_t)r * ncol + col] = acc[q][v];
-        }
-    }
+    dmma_tile(
+        n, ncol, kb, ke, blockIdx.y * DG_BM, blockIdx.x * DG_BN,
+        [&](int m, int k) { return __ldg(A + (size_t)m * n + k); },
+        [&](int c, int k) { return __ldg(BT + (size_t)c * n + k); },
+        [&](int m, int c, double v) { Cz[(size_t)m * ncol + c] = v; });
 }
 
 // out_c[m*nz + iz] = scale * sum_z Cp[z][m][c*nz + iz]  (slices in order)
@@ -399,7 +360,7 @@ int advect(cutcell_hill* H, const double* ux, const double* uy, const double* uz
     hill_gather_kernel<<<(d.nr + 7) / 8, 256, 0, s>>>(d, H->part, H->T);
     HCK(cudaGetLastError());
     const int ncol = 3 * d.nz;
-    dim3 g((d.nr + HG_T - 1) / HG_T, (ncol + HG_T - 1) / HG_T, HILL_KSPLIT);
+    dim3 g((ncol + DG_BN - 1) / DG_BN, (d.nr + DG_BM - 1) / DG_BM, HILL_KSPLIT);
     hill_gemm_kernel<<<g, 256, 0, s>>>(d.nr, ncol, d.M2inv, H->T, H->Cp);
     HCK(cudaGetLastError());
     hill_sum_kernel<<<296, 256, 0, s>>>(d.nr, d.nz, HILL_KSPLIT, H->Cp, scale, ox, oy, oz);

@@ -249,6 +249,7 @@ __host__ __device__ constexpr int sym64_index(int i, int j) {
 template <typename CT, int P1>
 struct TileOp {
     static constexpr bool kFusedP = true;
+    static constexpr int kDegree1 = P1;  // p + 1
     static constexpr int P = P1 * P1 * P1;
     static constexpr int PP = P1 * P1;
     static constexpr int T = 4;

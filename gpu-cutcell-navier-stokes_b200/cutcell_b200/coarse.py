@@ -59,13 +59,18 @@ def coarse_factor(n: int, degree: int, max_dofs: int = 2048) -> int:
     raise ValueError(f"no coarse grid of <= {max_dofs} functions for n = {n}, p = {degree}")
 
 
-def _bands(R: np.ndarray):
+def _bands(R: np.ndarray, pw: int | None = None):
     """Banded rows (plo, pw, pval) and columns (rlo, rw, rval) of R1, each
-    band start clamped so that start + width stays inside the grid."""
+    band start clamped so that start + width stays inside the grid.  ``pw``
+    pads the row bands to a given width (the device unrolls p + 1)."""
     nb, nbc = R.shape
     rows = [np.nonzero(R[x])[0] for x in range(nb)]
     cols = [np.nonzero(R[:, a])[0] for a in range(nbc)]
-    pw = max(int(ix[-1] - ix[0] + 1) for ix in rows if ix.size)
+    need = max(int(ix[-1] - ix[0] + 1) for ix in rows if ix.size)
+    if pw is None:
+        pw = need
+    if need > pw or pw > nbc:
+        raise ValueError(f"prolongation rows need a band of {need}; asked for {pw} on {nbc} coarse functions")
     rw = max(int(ix[-1] - ix[0] + 1) for ix in cols if ix.size)
     plo = np.array([min(int(ix[0]) if ix.size else 0, nbc - pw) for ix in rows], dtype=np.int32)
     rlo = np.array([min(int(ix[0]) if ix.size else 0, nb - rw) for ix in cols], dtype=np.int32)
@@ -117,7 +122,7 @@ class CoarseLevel:
         inv_k = 0.5 * (inv_k + inv_k.T)
         minv = np.zeros((self.ncg, self.ncg))
         minv[np.ix_(keep, keep)] = inv_k
-        plo, pw, pval, rlo, rw, rval = _bands(R)
+        plo, pw, pval, rlo, rw, rval = _bands(R, prob.degree + 1)
         self.pw, self.rw = pw, rw
         dv = op.device
         self._t = {

@@ -233,7 +233,7 @@ int cutcell_pcg_set_patch_blocks(cutcell_ctx* ctx, const int32_t* patch_red, int
  * per axis) restricted to the reduced DOFs, Ac = P^T A P, B the patch solves
  * of cutcell_pcg_set_patch_blocks (Jacobi on patches without a block).  The
  * 1D refinement is given twice, banded: by fine row x (coarse columns
- * plo[x] .. plo[x] + pw - 1, values pval[x][pw]) and by coarse column a
+ * plo[x] .. plo[x] + pw - 1, values pval[x][pw], pw = p + 1) and by coarse column a
  * (fine rows rlo[a] .. rlo[a] + rw - 1, values rval[a][rw]); zero entries pad
  * the bands.  minv is Ac^-1 on the full coarse grid (nbc^3 x nbc^3,
  * row-major, coarse index (c nbc + b) nbc + a for (x, y, z) = (a, b, c)), zero

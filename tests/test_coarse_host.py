@@ -37,6 +37,19 @@ def test_bands_reproduce_refinement():
     np.testing.assert_array_equal(Rp, R)
     np.testing.assert_array_equal(Rr, R)
     assert pw <= 4 and rw <= 13
+    # padded to p + 1 for the device's unrolled prolongation
+    plo4, pw4, pval4, *_ = _bands(R, 4)
+    assert pw4 == 4 and np.all(plo4 + 4 <= nbc)
+    for x in range(nb):
+        np.testing.assert_array_equal(R[x, plo4[x]:plo4[x] + 4], pval4[x])
+        assert np.count_nonzero(R[x]) == np.count_nonzero(pval4[x])
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("n,c", [(8, 2), (16, 2), (32, 4), (64, 8)])
+def test_prolongation_rows_fit_degree_plus_one(n, c, p):
+    R = refinement_1d(n, p, c)
+    _bands(R, p + 1)  # raises if a fine row needs a wider band
 
 
 def test_coarse_factor_rule():
