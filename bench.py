@@ -124,9 +124,12 @@ class ClockSampler:
 # command; None where no capture was made for that configuration.
 NCU_TRAFFIC = {
     ("sphere", 32, 3): 37.10e6 + 1.50e6,   # pcg_kernel, one whole solve
+    ("sphere-twolevel", 32, 3): 484.79e6 + 69.52e6,  # tlpcg_kernel, one whole solve
+    ("sphere-block", 32, 3): 131.61e6 + 7.13e6,      # ppcg_kernel (exact patch blocks), one whole solve
+    ("cut-box", 64, 3): 2.38e6,                      # apply_kernel<KronOp>, one apply
     ("apply", 64, 3): 157.17e6 + 6.61e6,   # apply_kernel, one apply
     ("batch", 72): 17.6e6,                 # batch_pcg_kernel, one launch
-    ("hill-step",): 161.7e6 + 32.6e6,      # hill_segment_kernel, one 3-component advection
+    ("hill-step",): 245.29e6 + 55.68e6,    # hill_segment_kernel, one 3-component advection (64x32x32 channel, single launch)
 }
 
 
@@ -166,6 +169,22 @@ def algorithmic_bytes_per_iter(prob, ext, prec: str) -> float:
     s = {"fp64": 8, "fp32-ir": 4, "bf16-ir": 4}[prec]  # bf16-ir: two BF16 planes per entry
     b_op = prob.cut_ids.size * cut_block_entries(prob.P) * s
     return 13 * 8 * N + b_e + b_op
+
+
+def algorithmic_bytes_patch(prob, ext, n_patch: int, ncg: int = 0) -> float:
+    """Per iteration of the patch-preconditioned solves: the FP64 operator
+    streams of one apply (B_E + B_op) once (exact blocks) or twice (two-level:
+    A p and A zc), the patch inverses (8 * 4096 bytes per patch), the dense
+    coarse inverse (8 ncg^2), and the FP64 vector streams (13 N for one
+    apply's PCG; the two-level form adds the line update, prolongation,
+    second apply and the split patch step: 20 N in all)."""
+    N = ext.n_red
+    nnz_small = int(ext.E[ext.small_support].nnz)
+    b_e = 2 * (4 + 8) * nnz_small + 4 * ext.n_full
+    b_op = prob.cut_ids.size * cut_block_entries(prob.P) * 8
+    if ncg:
+        return 2 * (b_e + b_op) + 20 * 8 * N + 8 * 4096 * n_patch + 8 * ncg * ncg
+    return (b_e + b_op) + 13 * 8 * N + 8 * 4096 * n_patch
 
 
 def cpu_baseline(prob, ext, b, sample_solves=1):
@@ -831,6 +850,24 @@ def main():
     hbm, hbm_kind = peaks()
     bytes_iter = algorithmic_bytes_per_iter(prob, ext, "fp64")
     achieved = bytes_iter * plain["iterations"] / (plain["kernel_ms"] / 1e3) / 1e9
+    roof_plain = {"bound": "hbm", "kernel": "pcg_kernel<TileOp<double>> (plain FP64, whole solve)",
+                  "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
+                  "traffic": NCU_TRAFFIC.get(("sphere", args.n, args.p)), "traffic_per": "launch (one solve)",
+                  "bytes_per_iter": bytes_iter}
+    # the roofline of the headline variant's kernel
+    roof = roof_plain
+    if best_key in ("twolevel", "block") and hasattr(op, "_patches"):
+        npatch = int(op._patches.n_patch)
+        ncg = int(op._coarse.ncg) if best_key == "twolevel" else 0
+        b_it = algorithmic_bytes_patch(prob, ext, npatch, ncg)
+        ach = b_it * best["iterations"] / (best["kernel_ms"] / 1e3) / 1e9
+        roof = {"bound": "hbm",
+                "kernel": ("tlpcg_kernel<TileOp<double,4>> (two-level flexible PCG, whole solve)" if best_key == "twolevel"
+                           else "ppcg_kernel<TileOp<double,4>> (exact patch blocks, whole solve)"),
+                "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "peak_kind": hbm_kind,
+                "traffic": NCU_TRAFFIC.get(("sphere-" + best_key, args.n, args.p)), "traffic_per": "launch (one solve)",
+                "bytes_per_iter": b_it,
+                "note": "algorithmic bytes mostly served from L2 (traffic = ncu DRAM bytes of one launch)"}
     line = {
         "metric": METRIC,
         "value": best["s_per_solve"],
@@ -860,18 +897,8 @@ def main():
         "clocks": plain.get("clocks"),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(8 * ext.n_red), "d2h_bytes_per_step": int(8 * ext.n_red), "variant": e2e_prec},
         "gpu_launches": int(args.steps),
-        "roofline": {
-            "bound": "hbm",
-            "kernel": "pcg_kernel<TileOp<double>> (plain FP64, whole solve)",
-            "achieved": achieved,
-            "peak": hbm,
-            "unit": "GB/s",
-            "frac": achieved / hbm,
-            "peak_kind": hbm_kind,
-            "traffic": NCU_TRAFFIC.get(("sphere", args.n, args.p)),
-            "traffic_per": "launch (one solve)",
-            "bytes_per_iter": bytes_iter,
-        },
+        "roofline": roof,
+        "roofline_plain_fp64": roof_plain,
     }
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         A, cpu_s, cpu_it, xc = cpu_baseline(prob, ext, b_host)
@@ -942,9 +969,10 @@ def run_cutbox(args, dev, steps: int, n: int = 64, p: int = 3, warmup: int = 3):
         "workload": f"tensor cut box p={p} n={n} fractions (0.6,0.6,0.6), weak-penalty Poisson, Kronecker operator",
         "n_red": N, "iterations": int(rep.iterations), "converged": bool(rep.status == 0),
         "s_per_solve": float(np.mean(ms)) / 1e3, "apply_us": am * 1e3, "setup_s": setup_s,
-        "roofline_apply": {"bound": "hbm", "achieved": bytes_apply / (am * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+        "roofline_apply": {"bound": "hbm", "kernel": "apply_kernel<KronOp>",
+                           "achieved": bytes_apply / (am * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                            "frac": bytes_apply / (am * 1e-3) / 1e9 / hbm, "peak_kind": hbm_kind,
-                           "algorithmic_bytes": bytes_apply},
+                           "algorithmic_bytes": bytes_apply, "traffic": NCU_TRAFFIC.get(("cut-box", n, p))},
     }
 
 

@@ -13,10 +13,12 @@
 //   restriction  P^T r : the x-contraction is fused into the x / r update
 //                        (one warp per x-line of the background grid), the
 //                        y-z contraction is one warp per coarse DOF;
-//   prolongation P y   : each reduced DOF sums its <= pw^3 coarse terms from
-//                        the coarse vector staged in shared memory, fused into
-//                        phase 0 of the apply A zc (its small rows of E zc are
-//                        formed from the same formula).
+//   prolongation P y   : each reduced DOF sums its (p + 1)^3 coarse terms
+//                        from the coarse vector staged in shared memory, in
+//                        its own phase before the apply A zc.  (Fusing it into
+//                        the apply's phase 0 saves a grid barrier but makes the
+//                        small rows of E zc re-evaluate the prolongation per
+//                        entry; measured 1.5 us per iteration slower at n = 32.)
 // Every sum has a fixed order; results are bit-reproducible.
 #pragma once
 
@@ -150,50 +152,52 @@ __device__ __forceinline__ void tl_coarse_solve(const CoarseDev& cd, double* srb
     __syncthreads();
     for (int row = gw; row < ncg; row += nw) {
         const double* m = cd.minv + (size_t)row * ncg;
-        double s = 0.0;
-        for (int col = lane; col < ncg; col += 32) s += __ldg(m + col) * srb[col];
-        s = warp_sum(s);
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // four chains: more row loads in flight
+        int col = lane;
+        for (; col + 96 < ncg; col += 128) {
+            s0 += __ldg(m + col) * srb[col];
+            s1 += __ldg(m + col + 32) * srb[col + 32];
+            s2 += __ldg(m + col + 64) * srb[col + 64];
+            s3 += __ldg(m + col + 96) * srb[col + 96];
+        }
+        for (; col < ncg; col += 32) s0 += __ldg(m + col) * srb[col];
+        double s = warp_sum((s0 + s1) + (s2 + s3));
         if (lane == 0) cd.yc[row] = s;
     }
     __syncthreads();
 }
 
-// One patch of the two-level step, by one warp: r' = r - A zc on the patch,
-// z = zc + B_P r' (exact block, or Jacobi), and this lane's shares of r.z and
-// r_old.z.
-__device__ __forceinline__ void tl_patch_step(const LearnedArgs& L, const CoarseDev& cd, const PcgBufs& B, int k,
-                                              double& rz, double& roz) {
+// Half h of patch k of the two-level step, by one warp (two warps per patch,
+// lane l owns patch row 32 h + l): r' = r - A zc on the patch (both halves,
+// for the block product), z = zc + B_P r' on this half (exact block, or
+// Jacobi), and this lane's shares of r.z and r_old.z.
+__device__ __forceinline__ void tl_patch_half(const LearnedArgs& L, const CoarseDev& cd, const PcgBufs& B, int k,
+                                              int h, double& rz, double& roz) {
     const int l = threadIdx.x & 31;
     const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
-    const double r0 = j0 >= 0 ? __ldcg(B.r + j0) : 0.0, r1 = j1 >= 0 ? __ldcg(B.r + j1) : 0.0;
-    const double q0 = j0 >= 0 ? r0 - __ldcg(cd.azc + j0) : 0.0, q1 = j1 >= 0 ? r1 - __ldcg(cd.azc + j1) : 0.0;
+    const double q0 = j0 >= 0 ? __ldcg(B.r + j0) - __ldcg(cd.azc + j0) : 0.0;
+    const double q1 = j1 >= 0 ? __ldcg(B.r + j1) - __ldcg(cd.azc + j1) : 0.0;
+    const int j = h ? j1 : j0;
+    const int row = 32 * h + l;
     const int slot = L.pm.slot ? __ldg(L.pm.slot + k) : -1;
-    double w0, w1;
-    if (slot >= 0 && L.pm.binv) {  // exact block solve, columns read coalesced (the inverse is symmetric)
-        const double* Bk = L.pm.binv + (size_t)slot * 4096;
-        w0 = 0.0;
-        w1 = 0.0;
-#pragma unroll 8
-        for (int q = 0; q < 64; ++q) {
-            const double rq = __shfl_sync(0xffffffffu, q < 32 ? q0 : q1, q & 31);
-            w0 += __ldg(Bk + q * 64 + l) * rq;
-            w1 += __ldg(Bk + q * 64 + l + 32) * rq;
+    double w;
+    if (slot >= 0 && L.pm.binv) {  // exact block solve: column q of the symmetric inverse is row q
+        const double* Bk = L.pm.binv + (size_t)slot * 4096 + row;
+        double w0 = 0.0, w1 = 0.0;
+#pragma unroll 16
+        for (int q = 0; q < 32; ++q) {
+            w0 += __ldg(Bk + q * 64) * __shfl_sync(0xffffffffu, q0, q);
+            w1 += __ldg(Bk + (q + 32) * 64) * __shfl_sync(0xffffffffu, q1, q);
         }
+        w = w0 + w1;
     } else {
-        w0 = j0 >= 0 ? __ldg(B.dinv + j0) * q0 : 0.0;
-        w1 = j1 >= 0 ? __ldg(B.dinv + j1) * q1 : 0.0;
+        w = j >= 0 ? __ldg(B.dinv + j) * (h ? q1 : q0) : 0.0;
     }
-    if (j0 >= 0) {
-        const double z0 = __ldcg(cd.zc + j0) + w0;
-        L.z[j0] = z0;
-        rz += r0 * z0;
-        roz += __ldcg(L.rold + j0) * z0;
-    }
-    if (j1 >= 0) {
-        const double z1 = __ldcg(cd.zc + j1) + w1;
-        L.z[j1] = z1;
-        rz += r1 * z1;
-        roz += __ldcg(L.rold + j1) * z1;
+    if (j >= 0) {
+        const double zj = __ldcg(cd.zc + j) + w;
+        L.z[j] = zj;
+        rz += __ldcg(B.r + j) * zj;
+        roz += __ldcg(L.rold + j) * zj;
     }
 }
 
@@ -213,12 +217,16 @@ __device__ __forceinline__ bool tl_precond(const Op& op, const CoarseDev& cd, co
     if (!grid_sync(gs)) return false;
     for (int i = threadIdx.x; i < cd.ncg; i += blockDim.x) sm[i] = __ldcg(cd.yc + i);
     __syncthreads();
-    op.phase0_from(ProlongFn<Op::kDegree1>{cd, op.td.ext.full_of_red, sm}, cd.zc);
+    {
+        const ProlongFn<Op::kDegree1> f{cd, op.td.ext.full_of_red, sm};
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < op.td.ext.n_red; i += gridDim.x * blockDim.x)
+            cd.zc[i] = f(i);
+    }
     if (!grid_sync(gs)) return false;
-    (void)op.apply_tail(cd.zc, cd.azc, gs, sm);
+    (void)op.apply(cd.zc, cd.azc, gs, sm);
     if (grid_error(gs) || !grid_sync(gs)) return false;
     double rz = 0.0, roz = 0.0;
-    for (int q = gw; q < L.pm.n_patch; q += nw) tl_patch_step(L, cd, B, q, rz, roz);
+    for (int q = gw; q < 2 * L.pm.n_patch; q += nw) tl_patch_half(L, cd, B, q >> 1, q & 1, rz, roz);
     rz = block_sum(rz, sh);
     roz = block_sum(roz, sh);
     if (threadIdx.x == 0) {

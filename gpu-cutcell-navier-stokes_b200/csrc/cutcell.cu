@@ -289,7 +289,10 @@ template <class Op>
 static int run_fcg(cutcell_ctx* c, const Op& op, size_t op_smem, SolveArgs& a, cudaStream_t s, int* blocks,
                    int mode) {
     const size_t op_al = (op_smem + 15) & ~(size_t)15;
-    const size_t smem = op_al + MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 3 * 64) * sizeof(float);
+    // the network's weights and per-warp scratch only for the learned form
+    // (mode 1); the block form needs the operator's shared memory alone
+    const size_t smem =
+        op_al + (mode == 1 ? MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 3 * 64) * sizeof(float) : 0);
     LearnedArgs L;
     memset(&L, 0, sizeof(L));
     if (mode == 1) L.W = c->mlp->weights();
@@ -1021,10 +1024,11 @@ int cutcell_mlp_params(cutcell_mlp* m, float* theta_out, float* grad_out) {
 int cutcell_mlp_forward(cutcell_mlp* m, const float* X, int32_t batch, float* Y, void* stream) {
     if (!m || !X || !Y || batch < 0) return CUTCELL_E_ARG;
     if (batch == 0) return CUTCELL_OK;
-    const size_t smem = MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 3 * 64) * sizeof(float);
-    CK(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    mlp_forward_kernel<<<ceil_div(batch, CUTCELL_WARPS), CUTCELL_BLOCK, smem, (cudaStream_t)stream>>>(m->weights(), X,
-                                                                                                   batch, Y);
+    const size_t smem = MlpTcSmem::bytes();
+    CK(cudaFuncSetAttribute(mlp_forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int tiles = ceil_div(batch, 16);
+    const int nblk = std::min(ceil_div(tiles, MLPT_WARPS), 2 * 148);
+    mlp_forward_tc_kernel<<<nblk, MLPT_WARPS * 32, smem, (cudaStream_t)stream>>>(m->weights(), X, batch, Y);
     CK(cudaGetLastError());
     return CUTCELL_OK;
 }
@@ -1043,12 +1047,13 @@ int cutcell_mlp_train_step(cutcell_mlp* m, const float* X, const float* T, int32
         CK(cudaMalloc(&m->L, (size_t)batch * sizeof(float)));
         m->cap = batch;
     }
-    const size_t smem = MlpSmem::bytes() + (size_t)CUTCELL_WARPS * (MLP_IN + 6 * 64) * sizeof(float);
-    CK(cudaFuncSetAttribute(mlp_fwd_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int nblk = ceil_div(batch, CUTCELL_WARPS) < 4 * 148 ? ceil_div(batch, CUTCELL_WARPS) : 4 * 148;
-    mlp_fwd_bwd_kernel<<<nblk, CUTCELL_BLOCK, smem, s>>>(m->weights(), X, T, batch, m->H1, m->H2, m->D1, m->D2, m->DY,
-                                                        m->Y, m->L);
-    mlp_grad_kernel<<<ceil_div(MLP_NPARAM, 128), 128, 0, s>>>(X, m->H1, m->H2, m->D1, m->D2, m->DY, batch, m->grad);
+    const size_t smem = MlpTcSmem::bytes();
+    CK(cudaFuncSetAttribute(mlp_fwd_bwd_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int nblk = std::min(ceil_div(ceil_div(batch, 16), MLPT_WARPS), 2 * 148);
+    mlp_fwd_bwd_tc_kernel<<<nblk, MLPT_WARPS * 32, smem, s>>>(m->weights(), X, T, batch, m->H1, m->H2, m->D1, m->D2,
+                                                             m->DY, m->Y, m->L);
+    mlp_wgrad_tc_kernel<<<4, 128, 0, s>>>(X, m->H1, m->H2, m->D1, m->D2, m->DY, batch, m->grad);
+    mlp_bgrad_kernel<<<1, 192, 0, s>>>(m->D1, m->D2, m->DY, batch, m->grad);
     if (loss_out) sum_in_order_kernel<<<1, CUTCELL_BLOCK, 0, s>>>(m->L, batch, 1.0f / (float)((long)batch * 64), loss_out);
     if (lr > 0.f) {
         m->step += 1;

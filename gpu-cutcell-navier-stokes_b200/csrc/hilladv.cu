@@ -22,6 +22,7 @@
 // Segment partials are summed per reduced mode in a fixed order (no atomics,
 // bit-reproducible), then the separable mass solve applies Mz^-1 per mode and
 // M2^-1 by a split-K FP64 GEMM.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -66,14 +67,17 @@ struct HillAdvDev {
 // Dynamic shared memory: the segment's coefficient rows C[a][comp][iz]
 // (lmax x 3 x nz), per warp two 9 x nz buffers, and the z tables (basis
 // values, derivatives, weights of every z element, laid out lane-contiguous).
+// CTA b takes segment seg_list[b]: segments are launched in two groups, the
+// ones of at most 16 modes with LMAX = 16 (a smaller CTA, four per SM) and
+// the longer ones with the next LMAX.
 template <int LMAX>
-__global__ void __launch_bounds__(HILL_WARPS * 32, 4) hill_segment_kernel(HillAdvDev d, const double* ux,
-                                                                      const double* uy, const double* uz,
-                                                                      double* part) {
+__global__ void __launch_bounds__(HILL_WARPS * 32, 4) hill_segment_kernel(HillAdvDev d, const int* seg_list,
+                                                                      const double* ux, const double* uy,
+                                                                      const double* uz, double* part) {
     constexpr int LW = (LMAX + HILL_WARPS - 1) / HILL_WARPS;  // modes owned per warp
     extern __shared__ double hs[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = blockIdx.x;
+    const int s = __ldg(seg_list + blockIdx.x);
     const int nz = d.nz;
     double* Cs = hs;
     double* Tw = Cs + LMAX * 3 * nz + w * 18 * nz;
@@ -341,7 +345,11 @@ struct cutcell_hill {
     double* T = nullptr;     // [nr][3 nz]
     double* Cp = nullptr;    // [KSPLIT][nr][3 nz]
     double* work = nullptr;  // 3 stage fields x 3 comps + 3 operator outputs: 12 x nr x nz
-    size_t smem = 0;
+    int* seg_list = nullptr;  // segments of <= 16 modes, then the longer ones
+    int n_short = 0;
+    int lm_long = 16;         // LMAX of the longer group
+    size_t smem_short = 0;    // dynamic shared memory of the LMAX = 16 group
+    size_t smem = 0;          // ... and of the longer group
 };
 
 namespace {
@@ -349,13 +357,16 @@ namespace {
 int advect(cutcell_hill* H, const double* ux, const double* uy, const double* uz, double scale, double* ox,
            double* oy, double* oz, cudaStream_t s) {
     const HillAdvDev& d = H->d;
-    const int blocks = d.n_seg;
-    if (d.lmax <= 16)
-        hill_segment_kernel<16><<<blocks, HILL_WARPS * 32, H->smem, s>>>(d, ux, uy, uz, H->part);
-    else if (d.lmax <= 24)
-        hill_segment_kernel<24><<<blocks, HILL_WARPS * 32, H->smem, s>>>(d, ux, uy, uz, H->part);
-    else
-        hill_segment_kernel<32><<<blocks, HILL_WARPS * 32, H->smem, s>>>(d, ux, uy, uz, H->part);
+    const int n_long = d.n_seg - H->n_short;
+    const int* longs = H->seg_list + H->n_short;
+    if (H->n_short > 0)
+        hill_segment_kernel<16><<<H->n_short, HILL_WARPS * 32, H->smem_short, s>>>(d, H->seg_list, ux, uy, uz, H->part);
+    if (n_long > 0) {
+        if (H->lm_long <= 24)
+            hill_segment_kernel<24><<<n_long, HILL_WARPS * 32, H->smem, s>>>(d, longs, ux, uy, uz, H->part);
+        else
+            hill_segment_kernel<32><<<n_long, HILL_WARPS * 32, H->smem, s>>>(d, longs, ux, uy, uz, H->part);
+    }
     HCK(cudaGetLastError());
     hill_gather_kernel<<<(d.nr + 7) / 8, 256, 0, s>>>(d, H->part, H->T);
     HCK(cudaGetLastError());
@@ -416,17 +427,41 @@ int cutcell_hill_create(const CutcellHillDesc* desc, cutcell_hill** out) {
     d.Mzinv = h.Mzinv;
     d.M2inv = h.M2inv;
     H->n_part = h.n_part;
-    const int lm = h.lmax <= 16 ? 16 : (h.lmax <= 24 ? 24 : 32);
-    H->smem = sizeof(double) * ((size_t)lm * 3 * h.nz + (size_t)HILL_WARPS * 18 * h.nz +
-                                (size_t)h.nz * h.qpe * (2 * HILL_NZB + 1));
+    auto smem_for = [&](int lm) {
+        return sizeof(double) * ((size_t)lm * 3 * h.nz + (size_t)HILL_WARPS * 18 * h.nz +
+                                 (size_t)h.nz * h.qpe * (2 * HILL_NZB + 1));
+    };
     const size_t fld = (size_t)h.nr * h.nz;
     cudaError_t e = cudaGetDevice(&H->device);
+    // segment groups by pattern length (host copy of seg_len)
+    std::vector<int> len(h.n_seg), order;
+    if (e == cudaSuccess) e = cudaMemcpy(len.data(), h.seg_len, sizeof(int) * h.n_seg, cudaMemcpyDeviceToHost);
+    int lmax_long = 0;
+    for (int i = 0; i < h.n_seg && e == cudaSuccess; ++i)
+        if (len[i] <= 16) order.push_back(i);
+    H->n_short = (int)order.size();
+    for (int i = 0; i < h.n_seg && e == cudaSuccess; ++i)
+        if (len[i] > 16) {
+            order.push_back(i);
+            lmax_long = std::max(lmax_long, len[i]);
+        }
+    if (e == cudaSuccess && (int)order.size() != h.n_seg) e = cudaErrorInvalidValue;
+    if (e == cudaSuccess && lmax_long > h.lmax) {
+        delete H;
+        return harg("hill: a segment pattern is longer than lmax", CUTCELL_E_SHAPE);
+    }
+    H->lm_long = lmax_long <= 24 ? 24 : 32;
+    H->smem_short = smem_for(16);
+    H->smem = smem_for(H->lm_long);
+    if (e == cudaSuccess) e = cudaMalloc(&H->seg_list, sizeof(int) * h.n_seg);
+    if (e == cudaSuccess) e = cudaMemcpy(H->seg_list, order.data(), sizeof(int) * h.n_seg, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&H->part, sizeof(double) * (size_t)h.n_part * 3 * h.nz);
     if (e == cudaSuccess) e = cudaMalloc(&H->T, sizeof(double) * fld * 3);
     if (e == cudaSuccess) e = cudaMalloc(&H->Cp, sizeof(double) * fld * 3 * HILL_KSPLIT);
     if (e == cudaSuccess) e = cudaMalloc(&H->work, sizeof(double) * fld * 12);
+    if (e == cudaSuccess && H->smem_short > 48 * 1024) e = (cudaError_t)set_smem<16>(H->smem_short);
     if (e == cudaSuccess && H->smem > 48 * 1024)
-        e = (cudaError_t)(lm == 16 ? set_smem<16>(H->smem) : (lm == 24 ? set_smem<24>(H->smem) : set_smem<32>(H->smem)));
+        e = (cudaError_t)(H->lm_long == 24 ? set_smem<24>(H->smem) : set_smem<32>(H->smem));
     if (e != cudaSuccess) {
         const int st = hfail(e, "cutcell_hill_create");
         cutcell_hill_destroy(H);
@@ -475,6 +510,7 @@ int cutcell_hill_destroy(cutcell_hill* H) {
     cudaFree(H->T);
     cudaFree(H->Cp);
     cudaFree(H->work);
+    cudaFree(H->seg_list);
     delete H;
     return CUTCELL_OK;
 }

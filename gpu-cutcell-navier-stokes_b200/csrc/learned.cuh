@@ -110,111 +110,12 @@ __device__ __forceinline__ void mlp_forward_warp(const MlpSmem& S, const float* 
 }
 
 // ---------------------------------------------------------------------------
-// Training kernels (batch of samples, row-major [batch][features]).
+// Training and batched inference on the BF16 tensor cores: mlp_tc.cuh.
+// (mlp_forward_warp above, one sample per warp, serves the patch inference
+// inside the flexible PCG, where each warp holds one patch.)
 // ---------------------------------------------------------------------------
 
-// forward + per-sample backward: stores z1, z2, h1, h2 and the deltas
-// dz1, dz2, dy for the weight-gradient kernel; loss partial per sample.
-__global__ void __launch_bounds__(256) mlp_fwd_bwd_kernel(MlpWeights W, const float* X, const float* Tgt, int batch,
-                                                          float* H1, float* H2, float* D1, float* D2, float* DY,
-                                                          float* Y, float* sample_loss) {
-    extern __shared__ __align__(16) char smem[];
-    MlpSmem S = mlp_load_smem(W, smem);
-    float* scratch = reinterpret_cast<float*>(smem + MlpSmem::bytes());
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
-    float* xs = scratch + warp * (MLP_IN + 6 * 64);
-    float* h1 = xs + MLP_IN;
-    float* h2 = h1 + 64;
-    float* y = h2 + 64;
-    float* z1 = y + 64;
-    float* z2 = z1 + 64;
-    float* d = z2 + 64;
-    const __nv_bfloat16* W2 = S.w + MLP_IN * MLP_H;
-    const __nv_bfloat16* W3 = W2 + MLP_H * MLP_H;
-    const float scale = 2.0f / (float)((long)batch * MLP_OUT);
-    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
-    for (int b = gw; b < batch; b += nw) {
-        for (int i = l; i < MLP_IN; i += 32) xs[i] = X[(size_t)b * MLP_IN + i];
-        __syncwarp();
-        mlp_forward_warp(S, xs, h1, h2, y, z1, z2);
-        // dy = 2 (y - t) / (batch * n_out)
-        float loss = 0.f;
-        for (int o = l; o < MLP_OUT; o += 32) {
-            const float e = y[o] - Tgt[(size_t)b * MLP_OUT + o];
-            loss += e * e;
-            d[o] = scale * e;
-            DY[(size_t)b * MLP_OUT + o] = scale * e;
-            Y[(size_t)b * MLP_OUT + o] = y[o];
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
-        if (l == 0) sample_loss[b] = loss;
-        __syncwarp();
-        // dz2 = (dy W3^T) * (z2 > 0)
-        float g0 = 0.f, g1 = 0.f;
-        for (int o = 0; o < MLP_OUT; ++o) {
-            const float dyo = d[o];
-            g0 = fmaf(dyo, __bfloat162float(W3[l * MLP_OUT + o]), g0);
-            g1 = fmaf(dyo, __bfloat162float(W3[(l + 32) * MLP_OUT + o]), g1);
-        }
-        g0 *= mlp_dact(z2[l], S.act);
-        g1 *= mlp_dact(z2[l + 32], S.act);
-        __syncwarp();
-        d[l] = g0;
-        d[l + 32] = g1;
-        D2[(size_t)b * 64 + l] = g0;
-        D2[(size_t)b * 64 + l + 32] = g1;
-        H2[(size_t)b * 64 + l] = h2[l];
-        H2[(size_t)b * 64 + l + 32] = h2[l + 32];
-        __syncwarp();
-        // dz1 = (dz2 W2^T) * (z1 > 0)
-        g0 = 0.f;
-        g1 = 0.f;
-        for (int o = 0; o < MLP_H; ++o) {
-            const float v = d[o];
-            g0 = fmaf(v, __bfloat162float(W2[l * MLP_H + o]), g0);
-            g1 = fmaf(v, __bfloat162float(W2[(l + 32) * MLP_H + o]), g1);
-        }
-        g0 *= mlp_dact(z1[l], S.act);
-        g1 *= mlp_dact(z1[l + 32], S.act);
-        D1[(size_t)b * 64 + l] = g0;
-        D1[(size_t)b * 64 + l + 32] = g1;
-        H1[(size_t)b * 64 + l] = h1[l];
-        H1[(size_t)b * 64 + l + 32] = h1[l + 32];
-        __syncwarp();
-    }
-}
-
-// Parameter gradients, one thread per parameter, samples summed in order.
-__global__ void mlp_grad_kernel(const float* X, const float* H1, const float* H2, const float* D1, const float* D2,
-                                const float* DY, int batch, float* grad) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= MLP_NPARAM) return;
-    const float* A;
-    const float* G;
-    int lda, ldg, i, o;
-    if (k < MLP_OFF_B1) {
-        i = k / MLP_H; o = k % MLP_H; A = X; lda = MLP_IN; G = D1; ldg = 64;
-    } else if (k < MLP_OFF_W2) {
-        i = -1; o = k - MLP_OFF_B1; A = nullptr; lda = 0; G = D1; ldg = 64;
-    } else if (k < MLP_OFF_B2) {
-        i = (k - MLP_OFF_W2) / MLP_H; o = (k - MLP_OFF_W2) % MLP_H; A = H1; lda = 64; G = D2; ldg = 64;
-    } else if (k < MLP_OFF_W3) {
-        i = -1; o = k - MLP_OFF_B2; A = nullptr; lda = 0; G = D2; ldg = 64;
-    } else if (k < MLP_OFF_B3) {
-        i = (k - MLP_OFF_W3) / MLP_OUT; o = (k - MLP_OFF_W3) % MLP_OUT; A = H2; lda = 64; G = DY; ldg = 64;
-    } else {
-        i = -1; o = k - MLP_OFF_B3; A = nullptr; lda = 0; G = DY; ldg = 64;
-    }
-    float s = 0.f;
-    if (A) {
-        for (int b = 0; b < batch; ++b) s = fmaf(A[(size_t)b * lda + i], G[(size_t)b * ldg + o], s);
-    } else {
-        for (int b = 0; b < batch; ++b) s += G[(size_t)b * ldg + o];
-    }
-    grad[k] = s;
-}
+#include "mlp_tc.cuh"
 
 // Adam step on the FP32 parameters and refresh of the BF16 weights.
 __global__ void mlp_adam_kernel(float* theta, float* m, float* v, const float* grad, __nv_bfloat16* wbf, float lr,
@@ -244,28 +145,6 @@ __global__ void mlp_refresh_bf16_kernel(const float* theta, __nv_bfloat16* wbf) 
     else if (k >= MLP_OFF_W2 && k < MLP_OFF_B2) w = MLP_IN * MLP_H + (k - MLP_OFF_W2);
     else if (k >= MLP_OFF_W3 && k < MLP_OFF_B3) w = MLP_IN * MLP_H + MLP_H * MLP_H + (k - MLP_OFF_W3);
     if (w >= 0) wbf[w] = __float2bfloat16(theta[k]);
-}
-
-// Inference over a batch (warp per sample).
-__global__ void __launch_bounds__(256) mlp_forward_kernel(MlpWeights W, const float* X, int batch, float* Y) {
-    extern __shared__ __align__(16) char smem[];
-    MlpSmem S = mlp_load_smem(W, smem);
-    float* scratch = reinterpret_cast<float*>(smem + MlpSmem::bytes());
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, l = threadIdx.x & 31;
-    float* xs = scratch + warp * (MLP_IN + 3 * 64);
-    float* h1 = xs + MLP_IN;
-    float* h2 = h1 + 64;
-    float* y = h2 + 64;
-    const int gw = blockIdx.x * (blockDim.x >> 5) + warp, nw = gridDim.x * (blockDim.x >> 5);
-    for (int b = gw; b < batch; b += nw) {
-        for (int i = l; i < MLP_IN; i += 32) xs[i] = X[(size_t)b * MLP_IN + i];
-        __syncwarp();
-        mlp_forward_warp(S, xs, h1, h2, y, nullptr, nullptr);
-        Y[(size_t)b * MLP_OUT + l] = y[l];
-        Y[(size_t)b * MLP_OUT + l + 32] = y[l + 32];
-        __syncwarp();
-    }
 }
 
 // ---------------------------------------------------------------------------

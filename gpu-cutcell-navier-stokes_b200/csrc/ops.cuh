@@ -124,22 +124,6 @@ struct ExtDev {
         }
     }
 
-    // psmall[s] = E[small s, :] v with v_j = f(j) evaluated on the fly (v is
-    // being written concurrently by the same phase)
-    template <class F>
-    __device__ __forceinline__ void small_rows_fn(const F& f) const {
-        const int lane = threadIdx.x & 31;
-        const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-        const int nw = (gridDim.x * blockDim.x) >> 5;
-        for (int s = gw; s < n_small; s += nw) {
-            double acc = 0.0;
-            const int k1 = __ldg(small_ptr + s + 1);
-            for (int k = __ldg(small_ptr + s) + lane; k < k1; k += 32) acc += __ldg(small_val + k) * f(__ldg(small_idx + k));
-            acc = warp_sum(acc);
-            if (lane == 0) psmall[s] = acc;
-        }
-    }
-
     // (E x)_i once small_rows(x) has completed grid-wide
     __device__ __forceinline__ double gather_fast(const double* x, int i) const {
         const int r = __ldg(red_of_full + i);
@@ -1113,16 +1097,6 @@ struct TileOp {
         td.ext.small_rows_next(pold, r, dinv, beta);
         if (!grid_sync(gs)) return 0.0;
         return apply_tail(pnew, y, gs, sm);
-    }
-
-    // Phase 0 of an apply to v_j = f(j): v written to vout for every reduced
-    // DOF and its small rows formed from f (the caller then syncs the grid
-    // and runs apply_tail(vout, ...)).
-    template <class F>
-    __device__ __forceinline__ void phase0_from(const F& f, double* vout) const {
-        const int n = td.ext.n_red;
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) vout[i] = f(i);
-        td.ext.small_rows_fn(f);
     }
 
     // phases 1-2b of the apply (phase 0 has completed grid-wide)

@@ -235,11 +235,13 @@ def z_element_tables(Vz, dVz, wz, nz):
     return zb, Vl, dVl, wzl, qpe
 
 
-def segment_tables(ptr, idx, seg_max=128):
+def segment_tables(ptr, idx, seg_max=128, long_pattern=16, seg_max_long=32):
     """Segments of consecutive 2D points whose sample rows have the same mode
-    pattern (at most seg_max points each), their patterns, and for every
-    reduced mode the partial rows (segment pattern slots) that feed it, in
-    segment order."""
+    pattern (at most seg_max points each; at most seg_max_long for patterns
+    longer than long_pattern modes, which the device runs as a separate,
+    smaller launch that should still spread over every SM), their patterns,
+    and for every reduced mode the partial rows (segment pattern slots) that
+    feed it, in segment order."""
     ptr = np.asarray(ptr, dtype=np.int64)
     idx = np.asarray(idx, dtype=np.int64)
     n2q = ptr.size - 1
@@ -247,8 +249,9 @@ def segment_tables(ptr, idx, seg_max=128):
     q = 0
     while q < n2q:
         pat = idx[ptr[q] : ptr[q + 1]]
+        cap = seg_max if pat.size <= long_pattern else seg_max_long
         r = q + 1
-        while r < n2q and r - q < seg_max and ptr[r + 1] - ptr[r] == pat.size and np.array_equal(idx[ptr[r] : ptr[r + 1]], pat):
+        while r < n2q and r - q < cap and ptr[r + 1] - ptr[r] == pat.size and np.array_equal(idx[ptr[r] : ptr[r + 1]], pat):
             r += 1
         q0s.append(q)
         q1s.append(r)
