@@ -182,9 +182,20 @@ def build_extension(
             out.append(cand[np.argsort(dist, kind="stable")])
         return out
 
-    for s0 in range(0, small.size, chunk):
-        blk = small[s0 : s0 + chunk]
-        order = nearest_order(blk)
+    # The neighbour orders of the chunks are independent and NumPy releases the
+    # GIL in the distance reductions and sorts, so they run on a thread pool;
+    # every row is the same computation as the sequential loop (bit-identical E).
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+
+    blocks = [small[s0 : s0 + chunk] for s0 in range(0, small.size, chunk)]
+    workers = max(1, min(8, os.cpu_count() or 1, len(blocks)))
+    if tree is None and workers > 1:
+        # a bound on the concurrent distance tables: chunk x interior x 4 doubles each
+        workers = max(1, min(workers, int(2.0e9 // max(1, chunk * interior.size * 32))))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        orders = list(pool.map(nearest_order, blocks))
+    for blk, order in zip(blocks, orders):
         for r, b in enumerate(blk):
             ordered = interior[order[r]]
             k = n_terms
