@@ -121,29 +121,38 @@ def test_kron_poisson_at_scale(torch_cuda):
         got = op.apply(x, form).cpu().numpy()
         assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref), form
     b = tb.poisson_rhs(box)
+    dinv = 1.0 / box.diag_A()
+
+    def host_pcg(tol):
+        """the same Jacobi-PCG on the host with the sum-factorised apply"""
+        xh = np.zeros_like(b)
+        r = b.copy()
+        z = dinv * r
+        pv = z.copy()
+        rz = r @ z
+        its = 0
+        for its in range(1, 20001):
+            Ap = _host_apply(box, "A", pv)
+            al = rz / (pv @ Ap)
+            xh += al * pv
+            r -= al * Ap
+            if np.linalg.norm(r) <= tol * np.linalg.norm(b):
+                break
+            z = dinv * r
+            rzn = r @ z
+            pv = z + (rzn / rz) * pv
+            rz = rzn
+        return xh, its
+
     xs, rep = solve_spd(op, b, tol=1e-10, maxiter=20000)
     assert rep.success, rep
-    # the same Jacobi-PCG on the host with the sum-factorised apply
-    dinv = 1.0 / box.diag_A()
-    xh = np.zeros_like(b)
-    r = b.copy()
-    z = dinv * r
-    pv = z.copy()
-    rz = r @ z
-    its = 0
-    for its in range(1, 20001):
-        Ap = _host_apply(box, "A", pv)
-        al = rz / (pv @ Ap)
-        xh += al * pv
-        r -= al * Ap
-        if np.linalg.norm(r) <= 1e-10 * np.linalg.norm(b):
-            break
-        z = dinv * r
-        rzn = r @ z
-        pv = z + (rzn / rz) * pv
-        rz = rzn
-    reph = {"iterations": its}
-    assert abs(reph["iterations"] - rep.iterations) <= max(1, 0.02 * rep.iterations)
+    _, its = host_pcg(1e-10)
+    assert abs(its - rep.iterations) <= max(1, 0.02 * rep.iterations)
+    # solutions compared at tol 1e-12: the ~950-iteration solves drift apart in
+    # rounding by about 1e-8 at tol 1e-10 (different summation orders)
+    xs, rep = solve_spd(op, b, tol=1e-12, maxiter=20000)
+    assert rep.success, rep
+    xh, _ = host_pcg(1e-12)
     assert np.linalg.norm(xs - xh) <= 1e-8 * np.linalg.norm(xh)
     op.close()
     torch.cuda.synchronize()
