@@ -171,7 +171,7 @@ def algorithmic_bytes_per_iter(prob, ext, prec: str) -> float:
     return 13 * 8 * N + b_e + b_op
 
 
-def algorithmic_bytes_patch(prob, ext, n_patch: int, ncg: int = 0) -> float:
+def algorithmic_bytes_patch(prob, ext, n_patch: int, ncg: int = 0, n_patch2: int = 0) -> float:
     """Per iteration of the patch-preconditioned solves: the FP64 operator
     streams of one apply (B_E + B_op) once (exact blocks) or twice (two-level:
     A p and A zc), the patch inverses (8 * 4096 bytes per patch), the dense
@@ -183,7 +183,8 @@ def algorithmic_bytes_patch(prob, ext, n_patch: int, ncg: int = 0) -> float:
     b_e = 2 * (4 + 8) * nnz_small + 4 * ext.n_full
     b_op = prob.cut_ids.size * cut_block_entries(prob.P) * 8
     if ncg:
-        return 2 * (b_e + b_op) + 20 * 8 * N + 8 * 4096 * n_patch + 8 * ncg * ncg
+        # the second tiling adds its inverses, z2 written and read, and r, A zc, r_old read again
+        return 2 * (b_e + b_op) + (20 + (5 if n_patch2 else 0)) * 8 * N + 8 * 4096 * (n_patch + n_patch2) + 8 * ncg * ncg
     return (b_e + b_op) + 13 * 8 * N + 8 * 4096 * n_patch
 
 
@@ -770,7 +771,9 @@ def main():
             t0 = time.perf_counter()
             cl = attach_coarse(op)
             t_coarse = {"setup_s": time.perf_counter() - t0, "galerkin_s": cl.galerkin_s, "factor": cl.factor,
-                        "coarse_dofs": int(cl.keep.size), "minv_bytes": int(8 * cl.ncg * cl.ncg)}
+                        "coarse_dofs": int(cl.keep.size), "minv_bytes": int(8 * cl.ncg * cl.ncg),
+                        "second_tiling_patches": int(cl.overlap.n_patch) if cl.overlap is not None else 0,
+                        "omega": cl.omega}
             solve_kw = {"precision": "fp64", "preconditioner": "twolevel"}
         elif prec in ("learned", "block"):
             from cutcell_b200.learned import attach_blocks
@@ -859,7 +862,8 @@ def main():
     if best_key in ("twolevel", "block") and hasattr(op, "_patches"):
         npatch = int(op._patches.n_patch)
         ncg = int(op._coarse.ncg) if best_key == "twolevel" else 0
-        b_it = algorithmic_bytes_patch(prob, ext, npatch, ncg)
+        ov = getattr(op._coarse, "overlap", None) if best_key == "twolevel" else None
+        b_it = algorithmic_bytes_patch(prob, ext, npatch, ncg, ov.n_patch if ov is not None else 0)
         ach = b_it * best["iterations"] / (best["kernel_ms"] / 1e3) / 1e9
         roof = {"bound": "hbm",
                 "kernel": ("tlpcg_kernel<TileOp<double,4>> (two-level flexible PCG, whole solve)" if best_key == "twolevel"

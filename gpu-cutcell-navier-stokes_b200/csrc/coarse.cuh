@@ -8,6 +8,9 @@
 // Galerkin coarse operator, inverted densely on the host (a few thousand
 // coarse DOFs, read from L2 every iteration).  Coarse correction first, patch
 // solves on the corrected residual: the two-grid cycle without pre-smoothing.
+// Optionally B = omega (B_0 + B_2) with a second patch tiling offset by 2
+// DOFs per axis; both tilings run in the same phase and keep their shares in
+// two vectors, summed by the next iteration's p update.
 //
 // The tensor structure of P is used in both directions:
 //   restriction  P^T r : the x-contraction is fused into the x / r update
@@ -37,6 +40,14 @@ struct CoarseDev {
     double* yc;                 // [ncg] Ac^-1 P^T r
     double* zc;                 // [n] P yc
     double* azc;                // [n] A zc
+    // optional second patch tiling, offset by 2 DOFs per axis:
+    //   z = zc + omega (B_0 + B_2) (r - A zc),
+    // with the B_2 share kept in z2 (n_patch2 = 0: z = zc + B_0 (r - A zc))
+    int n_patch2;
+    const int* red2;            // [n_patch2][64] reduced index or -1
+    const double* binv2;        // [n_patch2][64][64] symmetric patch inverses
+    double omega;
+    double* z2;                 // [n]
 };
 
 // zc_j = (P yc)_j from the coarse vector in shared memory.  PW = p + 1 is the
@@ -167,22 +178,26 @@ __device__ __forceinline__ void tl_coarse_solve(const CoarseDev& cd, double* srb
     __syncthreads();
 }
 
-// Half h of patch k of the two-level step, by one warp (two warps per patch,
-// lane l owns patch row 32 h + l): r' = r - A zc on the patch (both halves,
-// for the block product), z = zc + B_P r' on this half (exact block, or
-// Jacobi), and this lane's shares of r.z and r_old.z.
-__device__ __forceinline__ void tl_patch_half(const LearnedArgs& L, const CoarseDev& cd, const PcgBufs& B, int k,
-                                              int h, double& rz, double& roz) {
+// Half h of patch k of one tiling, by one warp (two warps per patch, lane l
+// owns patch row 32 h + l): r' = r - A zc on the patch (both halves, for the
+// block product), zout = zbase + wgt B_P r' on this half (exact block, or
+// Jacobi where the tiling has no block for the patch; zbase may be null), and
+// this lane's shares of r.zout and r_old.zout.  slot null with binv set means
+// block k for patch k.
+__device__ __forceinline__ void tl_patch_half(const int* red, const int* slot_map, const double* binv,
+                                              const double* zbase, double* zout, double wgt, const CoarseDev& cd,
+                                              const PcgBufs& B, const double* rold, int k, int h, double& rz,
+                                              double& roz) {
     const int l = threadIdx.x & 31;
-    const int j0 = __ldg(L.pm.red + (size_t)k * 64 + l), j1 = __ldg(L.pm.red + (size_t)k * 64 + l + 32);
+    const int j0 = __ldg(red + (size_t)k * 64 + l), j1 = __ldg(red + (size_t)k * 64 + l + 32);
     const double q0 = j0 >= 0 ? __ldcg(B.r + j0) - __ldcg(cd.azc + j0) : 0.0;
     const double q1 = j1 >= 0 ? __ldcg(B.r + j1) - __ldcg(cd.azc + j1) : 0.0;
     const int j = h ? j1 : j0;
     const int row = 32 * h + l;
-    const int slot = L.pm.slot ? __ldg(L.pm.slot + k) : -1;
+    const int slot = binv ? (slot_map ? __ldg(slot_map + k) : k) : -1;
     double w;
-    if (slot >= 0 && L.pm.binv) {  // exact block solve: column q of the symmetric inverse is row q
-        const double* Bk = L.pm.binv + (size_t)slot * 4096 + row;
+    if (slot >= 0) {  // exact block solve: column q of the symmetric inverse is row q
+        const double* Bk = binv + (size_t)slot * 4096 + row;
         double w0 = 0.0, w1 = 0.0;
 #pragma unroll 16
         for (int q = 0; q < 32; ++q) {
@@ -194,10 +209,10 @@ __device__ __forceinline__ void tl_patch_half(const LearnedArgs& L, const Coarse
         w = j >= 0 ? __ldg(B.dinv + j) * (h ? q1 : q0) : 0.0;
     }
     if (j >= 0) {
-        const double zj = __ldcg(cd.zc + j) + w;
-        L.z[j] = zj;
+        const double zj = (zbase ? __ldcg(zbase + j) : 0.0) + wgt * w;
+        zout[j] = zj;
         rz += __ldcg(B.r + j) * zj;
-        roz += __ldcg(L.rold + j) * zj;
+        roz += __ldcg(rold + j) * zj;
     }
 }
 
@@ -225,8 +240,18 @@ __device__ __forceinline__ bool tl_precond(const Op& op, const CoarseDev& cd, co
     if (!grid_sync(gs)) return false;
     (void)op.apply(cd.zc, cd.azc, gs, sm);
     if (grid_error(gs) || !grid_sync(gs)) return false;
+    // both tilings in one phase: each reduced DOF lies in one patch of each,
+    // and r.z = r.z_0 + r.z_2 is summed from the two tilings' shares
     double rz = 0.0, roz = 0.0;
-    for (int q = gw; q < 2 * L.pm.n_patch; q += nw) tl_patch_half(L, cd, B, q >> 1, q & 1, rz, roz);
+    const int n0 = 2 * L.pm.n_patch, n2 = 2 * cd.n_patch2;
+    const double w0 = cd.n_patch2 ? cd.omega : 1.0;
+    for (int q = gw; q < n0 + n2; q += nw) {
+        if (q < n0)
+            tl_patch_half(L.pm.red, L.pm.slot, L.pm.binv, cd.zc, L.z, w0, cd, B, L.rold, q >> 1, q & 1, rz, roz);
+        else
+            tl_patch_half(cd.red2, nullptr, cd.binv2, nullptr, cd.z2, cd.omega, cd, B, L.rold, (q - n0) >> 1,
+                          (q - n0) & 1, rz, roz);
+    }
     rz = block_sum(rz, sh);
     roz = block_sum(roz, sh);
     if (threadIdx.x == 0) {
@@ -275,14 +300,17 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) tlpcg_kernel(Op op, SolveArg
     }
     if (status != CUTCELL_E_BARRIER) {
         rz = grid_reduce(part + 3 * nb, nb, sh);
-        for (int i = gtid; i < n; i += gstride) B.p[i] = __ldcg(L.z + i);
+        for (int i = gtid; i < n; i += gstride)
+            B.p[i] = cd.n_patch2 ? __dadd_rn(__ldcg(L.z + i), __ldcg(cd.z2 + i)) : __ldcg(L.z + i);
         if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
     }
     double* P[2] = {B.p, B.p2};
     double beta = 0.0;
     for (k = 1; k <= a.maxiter && status != CUTCELL_E_BARRIER; ++k) {
         double* pk = P[(k - 1) & 1];
-        double pap = (k > 1) ? op.apply_next(P[k & 1], pk, L.z, L.ones, beta, B.Ap, gs, sm) : op.apply(pk, B.Ap, gs, sm);
+        double pap = (k == 1)        ? op.apply(pk, B.Ap, gs, sm)
+                     : cd.n_patch2 ? op.apply_next2(P[k & 1], pk, L.z, cd.z2, beta, B.Ap, gs, sm)
+                                   : op.apply_next(P[k & 1], pk, L.z, L.ones, beta, B.Ap, gs, sm);
         if (grid_error(gs)) {
             status = CUTCELL_E_BARRIER;
             break;

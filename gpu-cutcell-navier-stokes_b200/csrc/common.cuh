@@ -120,6 +120,12 @@ __device__ __forceinline__ double p_next(double dinv, double r, double beta, dou
     return __fma_rn(beta, pold, __dmul_rn(dinv, r));
 }
 
+// p_new = (z1 + z2) + beta p_old, one fixed rounding sequence (the two-level
+// form with two patch tilings keeps their corrections in two vectors)
+__device__ __forceinline__ double p_next2(double z1, double z2, double beta, double pold) {
+    return __fma_rn(beta, pold, __dadd_rn(z1, z2));
+}
+
 template <typename T> struct Conv;
 // ld: read-only global load; sld: shared-memory load, both widened to acc
 template <> struct Conv<double> {

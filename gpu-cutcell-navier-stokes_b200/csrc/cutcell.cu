@@ -196,6 +196,7 @@ struct cutcell_ctx {
     bool has_coarse = false;
     CoarseDev coarse = {};
     double* cwork = nullptr;  // t1 | rc | yc | zc | azc
+    double* cz2 = nullptr;    // the second tiling's correction
     // reduced-precision forms: residual-replacement factor and cap
     double inner_tol = 0.1;
     int inner_maxiter = 0;
@@ -984,7 +985,7 @@ int cutcell_ext_scatter(cutcell_ctx* c, const double* y_full, double* y_red, voi
 int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);  // cudaFree below waits for the work that may still use the buffers
-    void* bufs[] = {c->cwork, c->pslot_all, c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->cwork, c->cz2, c->pslot_all, c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
                     c->p,     c->p2,    c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -1185,6 +1186,29 @@ int cutcell_pcg_set_coarse(cutcell_ctx* c, const CutcellCoarseDesc* d) {
         CK(cudaMalloc(&c->rold, (size_t)c->n * sizeof(double)));
     }
     c->has_coarse = true;
+    return CUTCELL_OK;
+}
+
+int cutcell_pcg_set_overlap_blocks(cutcell_ctx* c, const int32_t* patch_red, int32_t n_patch, const double* binv,
+                                   double omega) {
+    if (!c || c->kind != KIND_TILES) return CUTCELL_E_ARG;
+    CoarseDev& cd = c->coarse;
+    if (!binv) {
+        cd.n_patch2 = 0;
+        cd.red2 = nullptr;
+        cd.binv2 = nullptr;
+        return CUTCELL_OK;
+    }
+    if (!patch_red || n_patch <= 0 || !(omega > 0.0 && omega <= 1.0)) {
+        g_last_error = "overlap blocks: a patch layout, its inverses and a weight in (0, 1]";
+        return CUTCELL_E_ARG;
+    }
+    if (!c->cz2) CK(cudaMalloc(&c->cz2, (size_t)c->n * sizeof(double)));
+    cd.n_patch2 = n_patch;
+    cd.red2 = patch_red;
+    cd.binv2 = binv;
+    cd.omega = omega;
+    cd.z2 = c->cz2;
     return CUTCELL_OK;
 }
 

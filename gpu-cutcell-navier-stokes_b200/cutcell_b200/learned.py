@@ -51,16 +51,21 @@ class PatchLayout:
     red: np.ndarray  # (n_patch, 64) int32 reduced index or -1
     gamma: np.ndarray  # (n_patch, 64) float32
     origin: np.ndarray | None = None  # (n_patch, 3) full-grid index of the patch's first DOF (x, y, z)
+    shift: int = 0  # the tiling's offset: patch (px, py, pz) holds DOFs 4 p - shift .. 4 p - shift + 3 per axis
 
     @property
     def n_patch(self) -> int:
         return self.red.shape[0]
 
 
-def patch_layout(op: CutCellOperator) -> PatchLayout:
+def patch_layout(op: CutCellOperator, shift: int = 0) -> PatchLayout:
+    """4x4x4 DOF patches of the background grid holding the reduced DOFs;
+    ``shift`` offsets the tiling by that many DOFs on every axis (shift 2 is
+    the second, overlapping tiling of the two-level form).  Every reduced DOF
+    lies in exactly one patch of a tiling."""
     prob, ext = op.problem, op.extension
     nb = prob.n_basis
-    npa = -(-nb // 4)
+    npa = -(-(nb + shift) // 4)
     red_of_full = ext.device_layout()["red_of_full"]
     gamma = np.clip(prob.gamma, 0.0, 1.0)
     d = np.arange(4)
@@ -68,15 +73,15 @@ def patch_layout(op: CutCellOperator) -> PatchLayout:
     for pz in range(npa):
         for py in range(npa):
             for px in range(npa):
-                gz, gy, gx = np.meshgrid(4 * pz + d, 4 * py + d, 4 * px + d, indexing="ij")
-                ok = (gx < nb) & (gy < nb) & (gz < nb)
+                gz, gy, gx = np.meshgrid(4 * pz + d - shift, 4 * py + d - shift, 4 * px + d - shift, indexing="ij")
+                ok = (gx >= 0) & (gy >= 0) & (gz >= 0) & (gx < nb) & (gy < nb) & (gz < nb)
                 g = np.where(ok, (gz * nb + gy) * nb + gx, 0).ravel()
                 r = np.where(ok.ravel(), red_of_full[g], -1).astype(np.int32)
                 if np.any(r >= 0):
                     reds.append(r)
                     gams.append(np.where(ok.ravel(), gamma[g], 0.0).astype(np.float32))
-                    orig.append((4 * px, 4 * py, 4 * pz))
-    return PatchLayout(np.stack(reds), np.stack(gams), np.asarray(orig, dtype=np.int64))
+                    orig.append((4 * px - shift, 4 * py - shift, 4 * pz - shift))
+    return PatchLayout(np.stack(reds), np.stack(gams), np.asarray(orig, dtype=np.int64), shift)
 
 
 def init_params(seed: int = 0) -> np.ndarray:
@@ -233,7 +238,8 @@ def patch_blocks(op: CutCellOperator, dp: "DevicePatches") -> np.ndarray:
     first = np.array([r[r >= 0][0] for r in lay.red])
     g = op.extension.interior[first]
     nb = prob.n_basis
-    pz, py, px = g // (nb * nb) // 4, (g // nb) % nb // 4, g % nb // 4
+    sh = lay.shift
+    pz, py, px = (g // (nb * nb) + sh) // 4, ((g // nb) % nb + sh) // 4, (g % nb + sh) // 4
     colour = torch.as_tensor((pz % 2) * 4 + (py % 2) * 2 + (px % 2), device=op.device)
     blocks = torch.zeros((lay.n_patch, 64, 64), dtype=torch.float64, device=op.device)
     v = torch.zeros(op.n, dtype=torch.float64, device=op.device)

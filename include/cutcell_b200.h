@@ -249,6 +249,14 @@ typedef struct {
     const double* minv;
 } CutcellCoarseDesc;
 int cutcell_pcg_set_coarse(cutcell_ctx* ctx, const CutcellCoarseDesc* desc);
+/* Second patch tiling of CUTCELL_PRECOND_TWOLEVEL: patch_red[n_patch][64]
+ * (reduced index or -1) of 4x4x4 patches offset by 2 DOFs per axis from the
+ * first tiling, binv[n_patch][64][64] their symmetric inverses.  With it the
+ * step is z = zc + omega (B_0 + B_2) (r - A zc), 0 < omega <= 1; every reduced
+ * DOF must lie in exactly one patch of each tiling.  Device pointers, kept by
+ * reference; binv NULL removes the tiling. */
+int cutcell_pcg_set_overlap_blocks(cutcell_ctx* ctx, const int32_t* patch_red, int32_t n_patch, const double* binv,
+                                   double omega);
 
 /* ---- periodic-hill fast diagonalisation (FastDiagHill, cpp/include/cut/hill_fastdiag.h:20-80) ----
  * create: the reduced 2D forms M2, Qx2, Qy2 (nr x nr, row-major), the z

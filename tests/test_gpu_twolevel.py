@@ -30,11 +30,13 @@ def torch_cuda():
     return torch
 
 
-def _twolevel_fcg_cpu(A, b, groups, P, tol, maxiter=5000):
+def _twolevel_fcg_cpu(A, b, groups, P, tol, maxiter=5000, groups2=None, omega=0.5):
     """Flexible PCG (Polak-Ribiere beta) with z = zc + B (r - A zc),
-    zc = P Ac^-1 P^T r, B the exact inverses of A on the patch index groups:
+    zc = P Ac^-1 P^T r, B the exact inverses of A on the patch index groups
+    (with groups2, the second tiling: z = zc + omega (B_0 + B_2) (r - A zc)):
     the device iteration restated with the assembled matrix."""
     invs = [np.linalg.inv(A[idx][:, idx].toarray()) for idx in groups]
+    invs2 = [np.linalg.inv(A[idx][:, idx].toarray()) for idx in groups2] if groups2 is not None else None
     keep = np.nonzero(np.diff(P.tocsc().indptr))[0]
     Pk = P.tocsc()[:, keep]
     Ac = (Pk.T @ A @ Pk).toarray()
@@ -46,7 +48,12 @@ def _twolevel_fcg_cpu(A, b, groups, P, tol, maxiter=5000):
         w = np.zeros_like(r)
         for idx, inv in zip(groups, invs):
             w[idx] = inv @ q[idx]
-        return zc + w
+        if invs2 is None:
+            return zc + w
+        w2 = np.zeros_like(r)
+        for idx, inv in zip(groups2, invs2):
+            w2[idx] = inv @ q[idx]
+        return zc + omega * (w + w2)
 
     bn = np.linalg.norm(b)
     x = np.zeros_like(b)
@@ -99,9 +106,12 @@ def test_twolevel_matches_cpu_and_beats_block(torch_cuda, n):
         assert np.abs(cl.Ac - Ac_ref).max() <= 1e-10 * np.abs(Ac_ref).max()
         x9, r9 = solve_spd(op, b, tol=1e-9, maxiter=5000, preconditioner="twolevel")
         assert r9.success, r9
-        lay = patch_layout(op)
-        groups = [row[row >= 0] for row in lay.red]
-        _, it_cpu = _twolevel_fcg_cpu(A, b, groups, cl.P, 1e-9)
+        groups = [row[row >= 0] for row in patch_layout(op).red]
+        groups2 = [row[row >= 0] for row in patch_layout(op, 2).red]
+        # every reduced DOF in exactly one patch of each tiling
+        for g in (groups, groups2):
+            assert np.array_equal(np.sort(np.concatenate(g)), np.arange(ext.n_red))
+        _, it_cpu = _twolevel_fcg_cpu(A, b, groups, cl.P, 1e-9, groups2=groups2, omega=cl.omega)
         assert abs(r9.iterations - it_cpu) <= max(2, 0.03 * it_cpu), (r9.iterations, it_cpu)
         x13, r13 = solve_spd(op, b, tol=1e-13, maxiter=5000, preconditioner="twolevel")
         assert r13.success, r13
