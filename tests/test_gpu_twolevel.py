@@ -7,10 +7,10 @@ sphere-cut p = 3 systems (needs a B200).
   the same iteration (exact patch inverses and Ac from the assembled matrix)
   within max(2, 3 %).
 * Its tol-1e-13 solution is within 1e-9 (relative L2) of the oracle CG's.
-* It needs at most 0.55 of the iterations of the exact patch solves alone
-  ("block"); measured 66 / 128 at n = 8, 42 / 152 at n = 16 and 71 / 210 at
-  n = 24 (the ratio is largest at n = 8, whose coarse grid has only n = 4
-  elements).
+* It needs at most 0.3 of the iterations of the exact patch solves alone
+  ("block"); measured with the second tiling 22 / 128 at n = 8, 27 / 150 at
+  n = 16 and 38 / 208 at n = 24.
+* Every reduced DOF lies in exactly one patch of each tiling.
 """
 
 from __future__ import annotations
@@ -122,6 +122,6 @@ def test_twolevel_matches_cpu_and_beats_block(torch_cuda, n):
         assert rb.success, rb
         print(f"n={n} factor={cl.factor} coarse={keep.size} twolevel {r9.iterations} (cpu {it_cpu}) "
               f"block {rb.iterations} err {err:.2e} {r9.device_ms:.2f} ms vs {rb.device_ms:.2f} ms")
-        assert r9.iterations <= 0.55 * rb.iterations
+        assert r9.iterations <= 0.3 * rb.iterations
     finally:
         op.close()
