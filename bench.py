@@ -171,20 +171,26 @@ def algorithmic_bytes_per_iter(prob, ext, prec: str) -> float:
     return 13 * 8 * N + b_e + b_op
 
 
-def algorithmic_bytes_patch(prob, ext, n_patch: int, ncg: int = 0, n_patch2: int = 0) -> float:
+def algorithmic_bytes_patch(prob, ext, n_patch: int, ncg: int = 0, extra_patches=()) -> float:
     """Per iteration of the patch-preconditioned solves: the FP64 operator
     streams of one apply (B_E + B_op) once (exact blocks) or twice (two-level:
-    A p and A zc), the patch inverses (8 * 4096 bytes per patch), the dense
-    coarse inverse (8 ncg^2), and the FP64 vector streams (13 N for one
-    apply's PCG; the two-level form adds the line update, prolongation,
-    second apply and the split patch step: 20 N in all)."""
+    A p and A zc), the patch inverses (4096 entries per patch: FP64 for the
+    exact-block form, FP32 for the two-level form, which also reads the
+    second tiling's), the dense coarse inverse (FP64, 8 ncg^2), and the FP64
+    vector streams (13 N for one apply's PCG; the two-level form adds the
+    line update, prolongation, second apply and the patch step: 20 N, and
+    6 N more per extra tiling: its z written and read twice, r, A zc and
+    r_old read again)."""
     N = ext.n_red
     nnz_small = int(ext.E[ext.small_support].nnz)
     b_e = 2 * (4 + 8) * nnz_small + 4 * ext.n_full
     b_op = prob.cut_ids.size * cut_block_entries(prob.P) * 8
     if ncg:
         # the second tiling adds its inverses, z2 written and read, and r, A zc, r_old read again
-        return 2 * (b_e + b_op) + (20 + (5 if n_patch2 else 0)) * 8 * N + 8 * 4096 * (n_patch + n_patch2) + 8 * ncg * ncg
+        # the two-level form stores its patch inverses in FP32, Ac^-1 in FP64
+        nx = len(extra_patches)
+        return (2 * (b_e + b_op) + (20 + 6 * nx) * 8 * N + 4 * 4096 * (n_patch + sum(extra_patches))
+                + 8 * ncg * ncg)
     return (b_e + b_op) + 13 * 8 * N + 8 * 4096 * n_patch
 
 
@@ -772,7 +778,7 @@ def main():
             cl = attach_coarse(op)
             t_coarse = {"setup_s": time.perf_counter() - t0, "galerkin_s": cl.galerkin_s, "factor": cl.factor,
                         "coarse_dofs": int(cl.keep.size), "minv_bytes": int(8 * cl.ncg * cl.ncg),
-                        "second_tiling_patches": int(cl.overlap.n_patch) if cl.overlap is not None else 0,
+                        "extra_tilings": {"shifts": list(cl.shifts), "patches": [int(t.n_patch) for t in cl.extra]},
                         "omega": cl.omega}
             solve_kw = {"precision": "fp64", "preconditioner": "twolevel"}
         elif prec in ("learned", "block"):
@@ -862,8 +868,8 @@ def main():
     if best_key in ("twolevel", "block") and hasattr(op, "_patches"):
         npatch = int(op._patches.n_patch)
         ncg = int(op._coarse.ncg) if best_key == "twolevel" else 0
-        ov = getattr(op._coarse, "overlap", None) if best_key == "twolevel" else None
-        b_it = algorithmic_bytes_patch(prob, ext, npatch, ncg, ov.n_patch if ov is not None else 0)
+        extra = [int(t.n_patch) for t in op._coarse.extra] if best_key == "twolevel" else []
+        b_it = algorithmic_bytes_patch(prob, ext, npatch, ncg, extra)
         ach = b_it * best["iterations"] / (best["kernel_ms"] / 1e3) / 1e9
         roof = {"bound": "hbm",
                 "kernel": ("tlpcg_kernel<TileOp<double,4>> (two-level flexible PCG, whole solve)" if best_key == "twolevel"

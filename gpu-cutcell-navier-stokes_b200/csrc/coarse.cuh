@@ -8,9 +8,10 @@
 // Galerkin coarse operator, inverted densely on the host (a few thousand
 // coarse DOFs, read from L2 every iteration).  Coarse correction first, patch
 // solves on the corrected residual: the two-grid cycle without pre-smoothing.
-// Optionally B = omega (B_0 + B_2) with a second patch tiling offset by 2
-// DOFs per axis; both tilings run in the same phase and keep their shares in
-// two vectors, summed by the next iteration's p update.
+// Optionally B = omega (B_0 + B_1 + ...) with up to three more patch tilings,
+// offset from the first by whole DOFs per axis; all tilings run in the same
+// phase and keep their shares in separate vectors, summed by the next
+// iteration's p update.
 //
 // The tensor structure of P is used in both directions:
 //   restriction  P^T r : the x-contraction is fused into the x / r update
@@ -40,14 +41,17 @@ struct CoarseDev {
     double* yc;                 // [ncg] Ac^-1 P^T r
     double* zc;                 // [n] P yc
     double* azc;                // [n] A zc
-    // optional second patch tiling, offset by 2 DOFs per axis:
-    //   z = zc + omega (B_0 + B_2) (r - A zc),
-    // with the B_2 share kept in z2 (n_patch2 = 0: z = zc + B_0 (r - A zc))
-    int n_patch2;
-    const int* red2;            // [n_patch2][64] reduced index or -1
-    const double* binv2;        // [n_patch2][64][64] symmetric patch inverses
+    // optional extra patch tilings (offset from the first):
+    //   z = zc + omega (B_0 + B_1 + ...) (r - A zc),
+    // tiling i's share kept in zx[i] (n_extra = 0: z = zc + B_0 (r - A zc))
+    int n_extra;
+    int n_patch_x[ZSUM_MAX];
+    const int* red_x[ZSUM_MAX];     // [n_patch_x][64] reduced index or -1
+    const float* binv_x[ZSUM_MAX];  // [n_patch_x][64][64] symmetric patch inverses (FP32 storage)
+    double* zx[ZSUM_MAX];           // [n] each
     double omega;
-    double* z2;                 // [n]
+    // FP32 copy of the first tiling's inverses (by block slot); null: its FP64 blocks
+    const float* binv0f;
 };
 
 // zc_j = (P yc)_j from the coarse vector in shared memory.  PW = p + 1 is the
@@ -183,8 +187,11 @@ __device__ __forceinline__ void tl_coarse_solve(const CoarseDev& cd, double* srb
 // block product), zout = zbase + wgt B_P r' on this half (exact block, or
 // Jacobi where the tiling has no block for the patch; zbase may be null), and
 // this lane's shares of r.zout and r_old.zout.  slot null with binv set means
-// block k for patch k.
-__device__ __forceinline__ void tl_patch_half(const int* red, const int* slot_map, const double* binv,
+// block k for patch k.  (Four warps per patch, 16 rows each with the columns
+// split over two lanes, measured slower: each item repeats the patch's r and
+// A zc loads.)
+template <typename BT>
+__device__ __forceinline__ void tl_patch_half(const int* red, const int* slot_map, const BT* binv,
                                               const double* zbase, double* zout, double wgt, const CoarseDev& cd,
                                               const PcgBufs& B, const double* rold, int k, int h, double& rz,
                                               double& roz) {
@@ -197,12 +204,12 @@ __device__ __forceinline__ void tl_patch_half(const int* red, const int* slot_ma
     const int slot = binv ? (slot_map ? __ldg(slot_map + k) : k) : -1;
     double w;
     if (slot >= 0) {  // exact block solve: column q of the symmetric inverse is row q
-        const double* Bk = binv + (size_t)slot * 4096 + row;
-        double w0 = 0.0, w1 = 0.0;
+        const BT* Bk = binv + (size_t)slot * 4096 + row;
+        double w0 = 0.0, w1 = 0.0;  // FP64 accumulation whatever the storage
 #pragma unroll 16
         for (int q = 0; q < 32; ++q) {
-            w0 += __ldg(Bk + q * 64) * __shfl_sync(0xffffffffu, q0, q);
-            w1 += __ldg(Bk + (q + 32) * 64) * __shfl_sync(0xffffffffu, q1, q);
+            w0 += (double)__ldg(Bk + q * 64) * __shfl_sync(0xffffffffu, q0, q);
+            w1 += (double)__ldg(Bk + (q + 32) * 64) * __shfl_sync(0xffffffffu, q1, q);
         }
         w = w0 + w1;
     } else {
@@ -243,14 +250,20 @@ __device__ __forceinline__ bool tl_precond(const Op& op, const CoarseDev& cd, co
     // both tilings in one phase: each reduced DOF lies in one patch of each,
     // and r.z = r.z_0 + r.z_2 is summed from the two tilings' shares
     double rz = 0.0, roz = 0.0;
-    const int n0 = 2 * L.pm.n_patch, n2 = 2 * cd.n_patch2;
-    const double w0 = cd.n_patch2 ? cd.omega : 1.0;
-    for (int q = gw; q < n0 + n2; q += nw) {
-        if (q < n0)
-            tl_patch_half(L.pm.red, L.pm.slot, L.pm.binv, cd.zc, L.z, w0, cd, B, L.rold, q >> 1, q & 1, rz, roz);
+    const int n0 = 2 * L.pm.n_patch;
+    int ntot = n0;
+    for (int i = 0; i < cd.n_extra; ++i) ntot += 2 * cd.n_patch_x[i];
+    const double w0 = cd.n_extra ? cd.omega : 1.0;
+    for (int q = gw; q < ntot; q += nw) {
+        if (q >= n0) {
+            int t = q - n0, i = 0;
+            while (i + 1 < cd.n_extra && t >= 2 * cd.n_patch_x[i]) t -= 2 * cd.n_patch_x[i++];
+            tl_patch_half(cd.red_x[i], (const int*)nullptr, cd.binv_x[i], nullptr, cd.zx[i], cd.omega, cd, B, L.rold,
+                          t >> 1, t & 1, rz, roz);
+        } else if (cd.binv0f)
+            tl_patch_half(L.pm.red, L.pm.slot, cd.binv0f, cd.zc, L.z, w0, cd, B, L.rold, q >> 1, q & 1, rz, roz);
         else
-            tl_patch_half(cd.red2, nullptr, cd.binv2, nullptr, cd.z2, cd.omega, cd, B, L.rold, (q - n0) >> 1,
-                          (q - n0) & 1, rz, roz);
+            tl_patch_half(L.pm.red, L.pm.slot, L.pm.binv, cd.zc, L.z, w0, cd, B, L.rold, q >> 1, q & 1, rz, roz);
     }
     rz = block_sum(rz, sh);
     roz = block_sum(roz, sh);
@@ -276,6 +289,10 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) tlpcg_kernel(Op op, SolveArg
     const int n = B.n, nb = gridDim.x;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
     double* lbuf = sm + (size_t)(threadIdx.x >> 5) * cd.nb;
+    ZSum zs;  // z = z_0 + the extra tilings' shares
+    zs.z0 = L.z;
+    zs.nx = cd.n_extra;
+    for (int i = 0; i < ZSUM_MAX; ++i) zs.zx[i] = cd.zx[i];
     double* part = B.part;
     const GridSync& gs = a.gs;
     double bb = 0.0;
@@ -300,17 +317,16 @@ __global__ void __launch_bounds__(CUTCELL_BLOCK, 2) tlpcg_kernel(Op op, SolveArg
     }
     if (status != CUTCELL_E_BARRIER) {
         rz = grid_reduce(part + 3 * nb, nb, sh);
-        for (int i = gtid; i < n; i += gstride)
-            B.p[i] = cd.n_patch2 ? __dadd_rn(__ldcg(L.z + i), __ldcg(cd.z2 + i)) : __ldcg(L.z + i);
+        for (int i = gtid; i < n; i += gstride) B.p[i] = zs.at(i);
         if (!grid_sync(gs)) status = CUTCELL_E_BARRIER;
     }
     double* P[2] = {B.p, B.p2};
     double beta = 0.0;
     for (k = 1; k <= a.maxiter && status != CUTCELL_E_BARRIER; ++k) {
         double* pk = P[(k - 1) & 1];
-        double pap = (k == 1)        ? op.apply(pk, B.Ap, gs, sm)
-                     : cd.n_patch2 ? op.apply_next2(P[k & 1], pk, L.z, cd.z2, beta, B.Ap, gs, sm)
-                                   : op.apply_next(P[k & 1], pk, L.z, L.ones, beta, B.Ap, gs, sm);
+        double pap = (k == 1)      ? op.apply(pk, B.Ap, gs, sm)
+                     : cd.n_extra ? op.apply_next_sum(P[k & 1], pk, zs, beta, B.Ap, gs, sm)
+                                  : op.apply_next(P[k & 1], pk, L.z, L.ones, beta, B.Ap, gs, sm);
         if (grid_error(gs)) {
             status = CUTCELL_E_BARRIER;
             break;

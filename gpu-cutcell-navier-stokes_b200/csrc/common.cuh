@@ -120,10 +120,24 @@ __device__ __forceinline__ double p_next(double dinv, double r, double beta, dou
     return __fma_rn(beta, pold, __dmul_rn(dinv, r));
 }
 
-// p_new = (z1 + z2) + beta p_old, one fixed rounding sequence (the two-level
-// form with two patch tilings keeps their corrections in two vectors)
-__device__ __forceinline__ double p_next2(double z1, double z2, double beta, double pold) {
-    return __fma_rn(beta, pold, __dadd_rn(z1, z2));
+// z = z0 + zx[0] + ... + zx[nx - 1], added in that order: the two-level form
+// keeps each patch tiling's correction in its own vector (every tiling writes
+// every reduced DOF, so they cannot share one within a phase)
+#define ZSUM_MAX 3
+struct ZSum {
+    const double* z0;
+    const double* zx[ZSUM_MAX];
+    int nx;
+    __device__ __forceinline__ double at(int j) const {
+        double s = __ldcg(z0 + j);
+        for (int i = 0; i < nx; ++i) s = __dadd_rn(s, __ldcg(zx[i] + j));
+        return s;
+    }
+};
+
+// p_new = z + beta p_old with z a ZSum, one fixed rounding sequence
+__device__ __forceinline__ double p_next_sum(const ZSum& z, int j, double beta, double pold) {
+    return __fma_rn(beta, pold, z.at(j));
 }
 
 template <typename T> struct Conv;

@@ -196,7 +196,7 @@ struct cutcell_ctx {
     bool has_coarse = false;
     CoarseDev coarse = {};
     double* cwork = nullptr;  // t1 | rc | yc | zc | azc
-    double* cz2 = nullptr;    // the second tiling's correction
+    double* czx[ZSUM_MAX] = {nullptr, nullptr, nullptr};  // the extra tilings' corrections
     // reduced-precision forms: residual-replacement factor and cap
     double inner_tol = 0.1;
     int inner_maxiter = 0;
@@ -985,7 +985,7 @@ int cutcell_ext_scatter(cutcell_ctx* c, const double* y_full, double* y_red, voi
 int cutcell_destroy(cutcell_ctx* c) {
     if (!c) return CUTCELL_E_ARG;
     cudaSetDevice(c->device);  // cudaFree below waits for the work that may still use the buffers
-    void* bufs[] = {c->cwork, c->cz2, c->pslot_all, c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
+    void* bufs[] = {c->cwork, c->czx[0], c->czx[1], c->czx[2], c->pslot_all, c->klo, c->kband, c->kscratch, c->val32, c->val16, c->cutsym, c->cut32, c->cut16, c->need_rec, c->row_rec, c->cut_pos, c->ypart, c->ycut, c->yfv, c->psmall, c->zl, c->rold, c->dinv, c->ones, c->r,
                     c->p,     c->p2,    c->Ap,    c->d,     c->rhat,  c->part,  c->bar,  c->res};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -1189,26 +1189,33 @@ int cutcell_pcg_set_coarse(cutcell_ctx* c, const CutcellCoarseDesc* d) {
     return CUTCELL_OK;
 }
 
-int cutcell_pcg_set_overlap_blocks(cutcell_ctx* c, const int32_t* patch_red, int32_t n_patch, const double* binv,
-                                   double omega) {
+int cutcell_pcg_set_twolevel_blocks(cutcell_ctx* c, const float* binv0, int32_t n_extra,
+                                    const int32_t* const* patch_red, const int32_t* n_patch, const float* const* binv,
+                                    double omega) {
     if (!c || c->kind != KIND_TILES) return CUTCELL_E_ARG;
     CoarseDev& cd = c->coarse;
-    if (!binv) {
-        cd.n_patch2 = 0;
-        cd.red2 = nullptr;
-        cd.binv2 = nullptr;
-        return CUTCELL_OK;
-    }
-    if (!patch_red || n_patch <= 0 || !(omega > 0.0 && omega <= 1.0)) {
-        g_last_error = "overlap blocks: a patch layout, its inverses and a weight in (0, 1]";
+    if (n_extra < 0 || n_extra > ZSUM_MAX || (n_extra > 0 && (!patch_red || !n_patch || !binv)) ||
+        (n_extra > 0 && !(omega > 0.0 && omega <= 1.0))) {
+        g_last_error = "two-level blocks: at most 3 extra tilings, each with a layout and inverses; weight in (0, 1]";
         return CUTCELL_E_ARG;
     }
-    if (!c->cz2) CK(cudaMalloc(&c->cz2, (size_t)c->n * sizeof(double)));
-    cd.n_patch2 = n_patch;
-    cd.red2 = patch_red;
-    cd.binv2 = binv;
-    cd.omega = omega;
-    cd.z2 = c->cz2;
+    for (int i = 0; i < n_extra; ++i)
+        if (!patch_red[i] || !binv[i] || n_patch[i] <= 0) {
+            g_last_error = "two-level blocks: an extra tiling without layout or inverses";
+            return CUTCELL_E_ARG;
+        }
+    for (int i = 0; i < n_extra; ++i)
+        if (!c->czx[i]) CK(cudaMalloc(&c->czx[i], (size_t)c->n * sizeof(double)));
+    cd.binv0f = binv0;
+    cd.n_extra = n_extra;
+    for (int i = 0; i < ZSUM_MAX; ++i) {
+        const bool on = i < n_extra;
+        cd.n_patch_x[i] = on ? n_patch[i] : 0;
+        cd.red_x[i] = on ? patch_red[i] : nullptr;
+        cd.binv_x[i] = on ? binv[i] : nullptr;
+        cd.zx[i] = c->czx[i];
+    }
+    cd.omega = n_extra > 0 ? omega : 1.0;
     return CUTCELL_OK;
 }
 

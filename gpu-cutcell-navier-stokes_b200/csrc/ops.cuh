@@ -124,10 +124,9 @@ struct ExtDev {
         }
     }
 
-    // psmall[s] = E[small s, :] p_new with p_new = (z1 + z2) + beta p_old
-    // formed on the fly (p_next2)
-    __device__ __forceinline__ void small_rows_next2(const double* pold, const double* z1, const double* z2,
-                                                     double beta) const {
+    // psmall[s] = E[small s, :] p_new with p_new = z + beta p_old formed on
+    // the fly (p_next_sum)
+    __device__ __forceinline__ void small_rows_next_sum(const double* pold, const ZSum& z, double beta) const {
         const int lane = threadIdx.x & 31;
         const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
         const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -136,7 +135,7 @@ struct ExtDev {
             const int k1 = __ldg(small_ptr + s + 1);
             for (int k = __ldg(small_ptr + s) + lane; k < k1; k += 32) {
                 const int j = __ldg(small_idx + k);
-                acc += __ldg(small_val + k) * p_next2(__ldcg(z1 + j), __ldcg(z2 + j), beta, __ldcg(pold + j));
+                acc += __ldg(small_val + k) * p_next_sum(z, j, beta, __ldcg(pold + j));
             }
             acc = warp_sum(acc);
             if (lane == 0) psmall[s] = acc;
@@ -1118,14 +1117,14 @@ struct TileOp {
         return apply_tail(pnew, y, gs, sm);
     }
 
-    // Phase 0 forms p_new = (z1 + z2) + beta p_old (p_next2) for every reduced
-    // DOF and its small rows from the same formula, then the apply.
-    __device__ __forceinline__ double apply_next2(const double* pold, double* pnew, const double* z1, const double* z2,
-                                                  double beta, double* y, const GridSync& gs, double* sm) const {
+    // Phase 0 forms p_new = z + beta p_old (p_next_sum, z a sum of vectors) for
+    // every reduced DOF and its small rows from the same formula, then the apply.
+    __device__ __forceinline__ double apply_next_sum(const double* pold, double* pnew, const ZSum& z, double beta,
+                                                     double* y, const GridSync& gs, double* sm) const {
         const int n = td.ext.n_red;
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-            pnew[i] = p_next2(__ldcg(z1 + i), __ldcg(z2 + i), beta, __ldcg(pold + i));
-        td.ext.small_rows_next2(pold, z1, z2, beta);
+            pnew[i] = p_next_sum(z, i, beta, __ldcg(pold + i));
+        td.ext.small_rows_next_sum(pold, z, beta);
         if (!grid_sync(gs)) return 0.0;
         return apply_tail(pnew, y, gs, sm);
     }

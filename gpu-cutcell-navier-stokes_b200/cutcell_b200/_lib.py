@@ -149,7 +149,7 @@ SIGNATURES = {
     "cutcell_pcg_set_block_inverses": (C.c_int, [_P, _P]),
     "cutcell_pcg_set_patch_blocks": (C.c_int, [_P, _P, C.c_int32, _P, _P]),
     "cutcell_pcg_set_coarse": (C.c_int, [_P, _P]),
-    "cutcell_pcg_set_overlap_blocks": (C.c_int, [_P, _P, C.c_int32, _P, C.c_double]),
+    "cutcell_pcg_set_twolevel_blocks": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P, C.c_double]),
     "cutcell_fastdiag_create": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     "cutcell_fastdiag_solve": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
     "cutcell_fastdiag_destroy": (C.c_int, [_P]),

@@ -60,8 +60,8 @@ class PatchLayout:
 
 def patch_layout(op: CutCellOperator, shift: int = 0) -> PatchLayout:
     """4x4x4 DOF patches of the background grid holding the reduced DOFs;
-    ``shift`` offsets the tiling by that many DOFs on every axis (shift 2 is
-    the second, overlapping tiling of the two-level form).  Every reduced DOF
+    ``shift`` offsets the tiling by that many DOFs on every axis (the extra,
+    overlapping tilings of the two-level form).  Every reduced DOF
     lies in exactly one patch of a tiling."""
     prob, ext = op.problem, op.extension
     nb = prob.n_basis

@@ -235,7 +235,7 @@ int cutcell_pcg_set_patch_blocks(cutcell_ctx* ctx, const int32_t* patch_red, int
  * 1D refinement is given twice, banded: by fine row x (coarse columns
  * plo[x] .. plo[x] + pw - 1, values pval[x][pw], pw = p + 1) and by coarse column a
  * (fine rows rlo[a] .. rlo[a] + rw - 1, values rval[a][rw]); zero entries pad
- * the bands.  minv is Ac^-1 on the full coarse grid (nbc^3 x nbc^3,
+ * the bands.  minv is Ac^-1 (FP64: the coarse solve is sensitive to its rounding) on the full coarse grid (nbc^3 x nbc^3,
  * row-major, coarse index (c nbc + b) nbc + a for (x, y, z) = (a, b, c)), zero
  * rows and columns for coarse functions without fluid.  All device pointers,
  * kept by reference; NULL desc removes the level.  At most 16384 coarse
@@ -249,14 +249,18 @@ typedef struct {
     const double* minv;
 } CutcellCoarseDesc;
 int cutcell_pcg_set_coarse(cutcell_ctx* ctx, const CutcellCoarseDesc* desc);
-/* Second patch tiling of CUTCELL_PRECOND_TWOLEVEL: patch_red[n_patch][64]
- * (reduced index or -1) of 4x4x4 patches offset by 2 DOFs per axis from the
- * first tiling, binv[n_patch][64][64] their symmetric inverses.  With it the
- * step is z = zc + omega (B_0 + B_2) (r - A zc), 0 < omega <= 1; every reduced
- * DOF must lie in exactly one patch of each tiling.  Device pointers, kept by
- * reference; binv NULL removes the tiling. */
-int cutcell_pcg_set_overlap_blocks(cutcell_ctx* ctx, const int32_t* patch_red, int32_t n_patch, const double* binv,
-                                   double omega);
+/* Patch inverses of CUTCELL_PRECOND_TWOLEVEL in FP32 storage (FP64
+ * accumulation).  binv0: the first tiling's inverses, indexed like the binv of
+ * cutcell_pcg_set_patch_blocks (NULL: use those FP64 blocks).  n_extra (0..3)
+ * more tilings, 4x4x4 patches offset from the first by whole DOFs per axis:
+ * host arrays of device pointers patch_red[i] ([n_patch[i]][64] reduced index
+ * or -1) and binv[i] ([n_patch[i]][64][64] symmetric inverses).  With them the
+ * step is z = zc + omega (B_0 + B_1 + ...) (r - A zc), 0 < omega <= 1, and
+ * every reduced DOF must lie in exactly one patch of each tiling.  The device
+ * pointers are kept by reference. */
+int cutcell_pcg_set_twolevel_blocks(cutcell_ctx* ctx, const float* binv0, int32_t n_extra,
+                                    const int32_t* const* patch_red, const int32_t* n_patch, const float* const* binv,
+                                    double omega);
 
 /* ---- periodic-hill fast diagonalisation (FastDiagHill, cpp/include/cut/hill_fastdiag.h:20-80) ----
  * create: the reduced 2D forms M2, Qx2, Qy2 (nr x nr, row-major), the z
