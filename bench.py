@@ -175,8 +175,8 @@ def algorithmic_bytes_patch(prob, ext, n_patch: int, ncg: int = 0, extra_patches
     """Per iteration of the patch-preconditioned solves: the FP64 operator
     streams of one apply (B_E + B_op) once (exact blocks) or twice (two-level:
     A p and A zc), the patch inverses (4096 entries per patch: FP64 for the
-    exact-block form, FP32 for the two-level form, which also reads the
-    second tiling's), the dense coarse inverse (FP64, 8 ncg^2), and the FP64
+    exact-block form, BF16 for the two-level form, which also reads the
+    extra tilings'), the dense coarse inverse (FP64, 8 ncg^2), and the FP64
     vector streams (13 N for one apply's PCG; the two-level form adds the
     line update, prolongation, second apply and the patch step: 20 N, and
     6 N more per extra tiling: its z written and read twice, r, A zc and
@@ -187,9 +187,9 @@ def algorithmic_bytes_patch(prob, ext, n_patch: int, ncg: int = 0, extra_patches
     b_op = prob.cut_ids.size * cut_block_entries(prob.P) * 8
     if ncg:
         # the second tiling adds its inverses, z2 written and read, and r, A zc, r_old read again
-        # the two-level form stores its patch inverses in FP32, Ac^-1 in FP64
+        # the two-level form stores its patch inverses in BF16, Ac^-1 in FP64
         nx = len(extra_patches)
-        return (2 * (b_e + b_op) + (20 + 6 * nx) * 8 * N + 4 * 4096 * (n_patch + sum(extra_patches))
+        return (2 * (b_e + b_op) + (20 + 6 * nx) * 8 * N + 2 * 4096 * (n_patch + sum(extra_patches))
                 + 8 * ncg * ncg)
     return (b_e + b_op) + 13 * 8 * N + 8 * 4096 * n_patch
 

@@ -47,11 +47,11 @@ struct CoarseDev {
     int n_extra;
     int n_patch_x[ZSUM_MAX];
     const int* red_x[ZSUM_MAX];     // [n_patch_x][64] reduced index or -1
-    const float* binv_x[ZSUM_MAX];  // [n_patch_x][64][64] symmetric patch inverses (FP32 storage)
+    const __nv_bfloat16* binv_x[ZSUM_MAX];  // [n_patch_x][64][64] symmetric patch inverses (BF16 storage)
     double* zx[ZSUM_MAX];           // [n] each
     double omega;
-    // FP32 copy of the first tiling's inverses (by block slot); null: its FP64 blocks
-    const float* binv0f;
+    // BF16 copy of the first tiling's inverses (by block slot); null: its FP64 blocks
+    const __nv_bfloat16* binv0h;
 };
 
 // zc_j = (P yc)_j from the coarse vector in shared memory.  PW = p + 1 is the
@@ -190,6 +190,10 @@ __device__ __forceinline__ void tl_coarse_solve(const CoarseDev& cd, double* srb
 // block k for patch k.  (Four warps per patch, 16 rows each with the columns
 // split over two lanes, measured slower: each item repeats the patch's r and
 // A zc loads.)
+// one stored patch-inverse entry, widened to FP64
+__device__ __forceinline__ double inv_entry(const double* p) { return __ldg(p); }
+__device__ __forceinline__ double inv_entry(const __nv_bfloat16* p) { return (double)__bfloat162float(__ldg(p)); }
+
 template <typename BT>
 __device__ __forceinline__ void tl_patch_half(const int* red, const int* slot_map, const BT* binv,
                                               const double* zbase, double* zout, double wgt, const CoarseDev& cd,
@@ -208,8 +212,8 @@ __device__ __forceinline__ void tl_patch_half(const int* red, const int* slot_ma
         double w0 = 0.0, w1 = 0.0;  // FP64 accumulation whatever the storage
 #pragma unroll 16
         for (int q = 0; q < 32; ++q) {
-            w0 += (double)__ldg(Bk + q * 64) * __shfl_sync(0xffffffffu, q0, q);
-            w1 += (double)__ldg(Bk + (q + 32) * 64) * __shfl_sync(0xffffffffu, q1, q);
+            w0 += inv_entry(Bk + q * 64) * __shfl_sync(0xffffffffu, q0, q);
+            w1 += inv_entry(Bk + (q + 32) * 64) * __shfl_sync(0xffffffffu, q1, q);
         }
         w = w0 + w1;
     } else {
@@ -260,8 +264,8 @@ __device__ __forceinline__ bool tl_precond(const Op& op, const CoarseDev& cd, co
             while (i + 1 < cd.n_extra && t >= 2 * cd.n_patch_x[i]) t -= 2 * cd.n_patch_x[i++];
             tl_patch_half(cd.red_x[i], (const int*)nullptr, cd.binv_x[i], nullptr, cd.zx[i], cd.omega, cd, B, L.rold,
                           t >> 1, t & 1, rz, roz);
-        } else if (cd.binv0f)
-            tl_patch_half(L.pm.red, L.pm.slot, cd.binv0f, cd.zc, L.z, w0, cd, B, L.rold, q >> 1, q & 1, rz, roz);
+        } else if (cd.binv0h)
+            tl_patch_half(L.pm.red, L.pm.slot, cd.binv0h, cd.zc, L.z, w0, cd, B, L.rold, q >> 1, q & 1, rz, roz);
         else
             tl_patch_half(L.pm.red, L.pm.slot, L.pm.binv, cd.zc, L.z, w0, cd, B, L.rold, q >> 1, q & 1, rz, roz);
     }

@@ -1189,9 +1189,9 @@ int cutcell_pcg_set_coarse(cutcell_ctx* c, const CutcellCoarseDesc* d) {
     return CUTCELL_OK;
 }
 
-int cutcell_pcg_set_twolevel_blocks(cutcell_ctx* c, const float* binv0, int32_t n_extra,
-                                    const int32_t* const* patch_red, const int32_t* n_patch, const float* const* binv,
-                                    double omega) {
+int cutcell_pcg_set_twolevel_blocks(cutcell_ctx* c, const uint16_t* binv0, int32_t n_extra,
+                                    const int32_t* const* patch_red, const int32_t* n_patch,
+                                    const uint16_t* const* binv, double omega) {
     if (!c || c->kind != KIND_TILES) return CUTCELL_E_ARG;
     CoarseDev& cd = c->coarse;
     if (n_extra < 0 || n_extra > ZSUM_MAX || (n_extra > 0 && (!patch_red || !n_patch || !binv)) ||
@@ -1206,13 +1206,13 @@ int cutcell_pcg_set_twolevel_blocks(cutcell_ctx* c, const float* binv0, int32_t 
         }
     for (int i = 0; i < n_extra; ++i)
         if (!c->czx[i]) CK(cudaMalloc(&c->czx[i], (size_t)c->n * sizeof(double)));
-    cd.binv0f = binv0;
+    cd.binv0h = reinterpret_cast<const __nv_bfloat16*>(binv0);
     cd.n_extra = n_extra;
     for (int i = 0; i < ZSUM_MAX; ++i) {
         const bool on = i < n_extra;
         cd.n_patch_x[i] = on ? n_patch[i] : 0;
         cd.red_x[i] = on ? patch_red[i] : nullptr;
-        cd.binv_x[i] = on ? binv[i] : nullptr;
+        cd.binv_x[i] = on ? reinterpret_cast<const __nv_bfloat16*>(binv[i]) : nullptr;
         cd.zx[i] = c->czx[i];
     }
     cd.omega = n_extra > 0 ? omega : 1.0;

@@ -249,8 +249,8 @@ typedef struct {
     const double* minv;
 } CutcellCoarseDesc;
 int cutcell_pcg_set_coarse(cutcell_ctx* ctx, const CutcellCoarseDesc* desc);
-/* Patch inverses of CUTCELL_PRECOND_TWOLEVEL in FP32 storage (FP64
- * accumulation).  binv0: the first tiling's inverses, indexed like the binv of
+/* Patch inverses of CUTCELL_PRECOND_TWOLEVEL in BF16 storage (uint16_t bit
+ * patterns of bfloat16; FP64 accumulation).  binv0: the first tiling's inverses, indexed like the binv of
  * cutcell_pcg_set_patch_blocks (NULL: use those FP64 blocks).  n_extra (0..3)
  * more tilings, 4x4x4 patches offset from the first by whole DOFs per axis:
  * host arrays of device pointers patch_red[i] ([n_patch[i]][64] reduced index
@@ -258,9 +258,9 @@ int cutcell_pcg_set_coarse(cutcell_ctx* ctx, const CutcellCoarseDesc* desc);
  * step is z = zc + omega (B_0 + B_1 + ...) (r - A zc), 0 < omega <= 1, and
  * every reduced DOF must lie in exactly one patch of each tiling.  The device
  * pointers are kept by reference. */
-int cutcell_pcg_set_twolevel_blocks(cutcell_ctx* ctx, const float* binv0, int32_t n_extra,
-                                    const int32_t* const* patch_red, const int32_t* n_patch, const float* const* binv,
-                                    double omega);
+int cutcell_pcg_set_twolevel_blocks(cutcell_ctx* ctx, const uint16_t* binv0, int32_t n_extra,
+                                    const int32_t* const* patch_red, const int32_t* n_patch,
+                                    const uint16_t* const* binv, double omega);
 
 /* ---- periodic-hill fast diagonalisation (FastDiagHill, cpp/include/cut/hill_fastdiag.h:20-80) ----
  * create: the reduced 2D forms M2, Qx2, Qy2 (nr x nr, row-major), the z
