@@ -124,7 +124,7 @@ class ClockSampler:
 # command; None where no capture was made for that configuration.
 NCU_TRAFFIC = {
     ("sphere", 32, 3): 37.10e6 + 1.50e6,   # pcg_kernel, one whole solve
-    ("sphere-twolevel", 32, 3): 2431.29e6 + 159.83e6,  # tlpcg_kernel (four patch tilings), one whole solve
+    ("sphere-twolevel", 32, 3): 410.43e6 + 42.31e6,  # tlpcg_kernel (four patch tilings, BF16 inverses), one whole solve
     ("sphere-block", 32, 3): 131.61e6 + 7.13e6,      # ppcg_kernel (exact patch blocks), one whole solve
     ("cut-box", 64, 3): 2.38e6,                      # apply_kernel<KronOp>, one apply
     ("apply", 64, 3): 157.17e6 + 6.61e6,   # apply_kernel, one apply
