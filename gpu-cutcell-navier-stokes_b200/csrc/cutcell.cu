@@ -1069,7 +1069,7 @@ int cutcell_mlp_train_step(cutcell_mlp* m, const float* X, const float* T, int32
 
 int cutcell_mlp_destroy(cutcell_mlp* m) {
     if (!m) return CUTCELL_E_ARG;
-    cudaDeviceSynchronize();
+    cudaSetDevice(m->device);  // cudaFree below waits for the work that may still use the buffers
     void* bufs[] = {m->theta, m->m, m->v, m->grad, m->wbf, m->H1, m->H2, m->D1, m->D2, m->DY, m->Y, m->L};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -1360,8 +1360,7 @@ int cutcell_fastdiag_solve(cutcell_fastdiag* f, const double* ux, const double* 
 
 int cutcell_fastdiag_destroy(cutcell_fastdiag* f) {
     if (!f) return CUTCELL_E_ARG;
-    cudaSetDevice(f->device);
-    cudaDeviceSynchronize();
+    cudaSetDevice(f->device);  // cudaFree below waits for the work that may still use the buffers
     void* bufs[] = {f->X, f->T, f->UT, f->G, f->U, f->S2, f->QxT, f->QyT, f->cosT, f->sinT, f->part};
     for (void* b : bufs)
         if (b) cudaFree(b);
