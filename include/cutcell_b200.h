@@ -390,8 +390,9 @@ int cutcell_batch_destroy(cutcell_batch* batch);
  * lives in one fixed file-scope device array of the library, sized for
  * n <= 65536 unknowns and <= 1024 persistent blocks (about 2.2 MB per GPU,
  * held until the process exits).  Larger n returns CUTCELL_E_SHAPE.  The
- * first call on each device resolves the array's address and the grid size;
- * make that first call before any stream capture.  Calls share the array:
+ * first call on each device resolves the array's address and the grid size.
+ * Every call copies the result to the host and synchronises its stream, so
+ * the call is not meant for stream capture.  Calls share the array:
  * calls that overlap on the GPU race and must be serialised by the caller.
  * The CSR structure is checked on the device first (as in
  * cutcell_pcg_create_csr); a malformed matrix returns CUTCELL_E_SHAPE
