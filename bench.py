@@ -100,22 +100,35 @@ class ClockSampler:
             self._stop.wait(0.2)
 
     def start(self):
+        """Starts sampling a timed region; a sampler may cover several regions in turn."""
+        self._stop.clear()
+        self._mark = len(self.rows)
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
 
     def stop(self):
+        """Ends the current region and returns the record of its samples."""
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+            self._t = None
+        return self.summary(self.rows[getattr(self, "_mark", 0):])
+
+    def total(self):
+        """The record of every region this sampler covered."""
+        return self.summary(self.rows)
+
+    @staticmethod
+    def summary(rows):
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i] and "Not" not in r[5 + i]})
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i] and "Not" not in r[5 + i]})
         return {
             "sm_mhz": float(np.median(sm)) if sm else None,
             "sm_max_mhz": float(max(mx)) if mx else None,
             "reasons": reasons,
-            "samples": len(self.rows),
+            "samples": len(rows),
         }
 
 
@@ -767,6 +780,9 @@ def main():
                         "canonical_patches": int(op._patch_solves.canonical.sum()) if hasattr(op, "_patch_solves") else None}
     t_blocks = None
     t_coarse = None
+    # one sampler over every variant's timed region (and only those): each
+    # variant keeps its own record, the line's record is the union
+    sampler = ClockSampler(local)
     for prec in wanted:
         solve_kw = {"precision": prec}
         if prec == "twolevel":
@@ -793,9 +809,7 @@ def main():
         for _ in range(args.warmup):
             x, rep = op.solve_device(b, tol=TOL, maxiter=20000, **solve_kw)
         barrier()
-        sampler = ClockSampler(local) if prec == "fp64" else None
-        if sampler:
-            sampler.start()
+        sampler.start()
         ms = []
         for _ in range(args.steps):
             flush.fill_(1.0)
@@ -807,7 +821,7 @@ def main():
             torch.cuda.synchronize(dev)
             ms.append(e0.elapsed_time(e1))
         barrier()
-        clocks = sampler.stop() if sampler else None
+        clocks = sampler.stop()
         tot = float(np.sum(ms))
         if world > 1:
             import torch.distributed as dist
@@ -904,7 +918,7 @@ def main():
             "setup_s": t_setup,
         },
         "variants": variants,
-        "clocks": plain.get("clocks"),
+        "clocks": dict(sampler.total(), regions="the timed solves of every variant"),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(8 * ext.n_red), "d2h_bytes_per_step": int(8 * ext.n_red), "variant": e2e_prec},
         "gpu_launches": int(args.steps),
         "roofline": roof,
