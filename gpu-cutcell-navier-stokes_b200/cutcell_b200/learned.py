@@ -261,7 +261,7 @@ def patch_colours(op: CutCellOperator, lay: PatchLayout) -> np.ndarray:
     cut cells the 8 parity colours already separate them.  A patch coupled to
     an earlier patch of its colour (through the extension rows of E) takes the
     smallest colour that none of its earlier coupled patches holds.  On the
-    sphere-cut p = 3 systems that gives 29-36 colours per tiling at n = 16 and
+    sphere-cut p = 3 systems that gives 26-33 colours per tiling at n = 16 and
     32-34 at n = 32."""
     K = patch_coupling(op, lay)
     if lay.origin is not None:
