@@ -174,3 +174,82 @@ def test_twolevel_iteration_on_the_host(p, device_its):
     # 1.6e-6 at p = 4)
     kappa = np.linalg.cond(A.toarray())
     assert np.linalg.norm(x - x_ref) <= 1e-9 * kappa * np.linalg.norm(x_ref)
+
+
+class _AssembledOp(_HostOp):
+    """An operator on the CPU whose apply is the oracle's assembled E^T A E."""
+
+    def __init__(self, prob, ext, A):
+        import torch
+
+        super().__init__(prob, ext)
+        self.A, self.device, self.n = A, torch.device("cpu"), ext.n_red
+
+    def apply(self, v):
+        import torch
+
+        return torch.as_tensor(self.A @ v.numpy())
+
+
+def test_twolevel_setup_data_on_the_host():
+    """The arrays the device receives, built on the CPU by the product's own
+    setup against the oracle's assembled E^T A E (sphere, n = 8, p = 3):
+    CoarseLevel's P and explicit FP64 Ac^-1, the first tiling's probed
+    inverses (symmetrised, BF16 as stored) and the extra tilings'
+    (OverlapTiling, BF16).  Flexible PCG with z = zc + 0.3 sum_i B_i (r - A zc)
+    from exactly those arrays takes the device's 18 iterations."""
+    import torch
+
+    from cutcell_b200.coarse import CoarseLevel, OverlapTiling
+    from cutcell_b200.learned import DevicePatches, patch_blocks, patch_inverses, patch_layout
+    from cutcell_b200.workloads import sphere_poisson
+    from oracle.aggregation import restrict_spd
+    from oracle.assembly import assemble_full
+
+    prob, ext = sphere_poisson(8, 3, 0.31)
+    A = restrict_spd(assemble_full(prob), ext.E).tocsr()
+    A = (0.5 * (A + A.T)).tocsr()
+    b = np.asarray(ext.E.T @ prob.load)
+    op = _AssembledOp(prob, ext, A)
+    cl = CoarseLevel(op)
+    lay0 = patch_layout(op, 0)
+    inv0 = patch_inverses(patch_blocks(op, DevicePatches(op, lay0)), lay0.red)
+    inv0 = 0.5 * (inv0 + np.transpose(inv0, (0, 2, 1)))
+    tilings = [(lay0.red, torch.as_tensor(inv0).to(torch.bfloat16).double().numpy())]
+    for shift in (1, 2, 3):
+        t = OverlapTiling(op, shift)
+        tilings.append((t.dp.layout.red, t.inv.double().numpy()))
+    minv = cl._t["minv"].numpy()
+    P = cl.P.tocsr()
+
+    def M(r):
+        zc = P @ (minv @ (P.T @ r))
+        q = r - A @ zc
+        w = np.zeros_like(r)
+        for red, inv in tilings:
+            for k in range(red.shape[0]):
+                m = red[k] >= 0
+                g = red[k][m]
+                w[g] += inv[k][np.ix_(m, m)] @ q[g]
+        return zc + 0.3 * w
+
+    x = np.zeros_like(b)
+    r = b.copy()
+    z = M(r)
+    pv = z.copy()
+    rz = r @ z
+    bn = np.linalg.norm(b)
+    its = 0
+    for its in range(1, 200):
+        Ap = A @ pv
+        al = rz / (pv @ Ap)
+        x += al * pv
+        rold = r.copy()
+        r -= al * Ap
+        if np.linalg.norm(r) <= 1e-9 * bn:
+            break
+        z = M(r)
+        beta = (r @ z - rold @ z) / rz
+        rz = r @ z
+        pv = z + beta * pv
+    assert its == 18, its
