@@ -269,7 +269,7 @@ def patch_colours(op: CutCellOperator, lay: PatchLayout) -> np.ndarray:
     else:
         nb = op.problem.n_basis
         g = op.extension.interior[np.array([r[r >= 0][0] for r in lay.red])]
-        pos = np.stack([g % nb, (g // nb) % nb, g // (nb * nb)], axis=1) // 4
+        pos = (np.stack([g % nb, (g // nb) % nb, g // (nb * nb)], axis=1) + lay.shift) // 4
     start = (pos[:, 2] % 2) * 4 + (pos[:, 1] % 2) * 2 + (pos[:, 0] % 2)
     colour = np.full(lay.n_patch, -1, dtype=np.int64)
     for k in range(lay.n_patch):
